@@ -1,0 +1,61 @@
+"""Loads libafrs_b200.so (built from csrc/ for sm_100a) and declares the C ABI
+of include/afrs.h for ctypes."""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libafrs_b200.so")
+
+AFRS_OK = 0
+AFRS_EINVAL = -1
+AFRS_ECUDA = -2
+AFRS_ENOMEM = -3
+AFRS_ETIMEOUT = -4
+
+_u8p = ctypes.c_void_p
+_sz = ctypes.c_size_t
+_u32 = ctypes.c_uint32
+
+# name -> (restype, argtypes); the list mirrors include/afrs.h.
+SIGNATURES = {
+    "afrs_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "afrs_ctx_destroy": (None, [ctypes.c_void_p]),
+    "afrs_last_error": (ctypes.c_char_p, []),
+    "afrs_version": (ctypes.c_char_p, []),
+    "afrs_encode": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _u8p, _sz, ctypes.c_int]),
+    "afrs_recover": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, _u8p, _sz]),
+    "afrs_encode_dev": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _u8p, _sz, ctypes.c_int, ctypes.c_void_p]),
+    "afrs_recover_dev": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, _u8p, _sz, ctypes.c_void_p]),
+    "afrs_recompute_data_from_parity_dev": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, ctypes.c_void_p]),
+    "afrs_fft_sharded_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _sz, _u32, ctypes.c_uint8, ctypes.c_void_p]),
+    "afrs_ifft_sharded_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _sz, _u32, ctypes.c_uint8, ctypes.c_void_p]),
+    "afrs_scale_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _u8p, _sz, ctypes.c_uint8, ctypes.c_void_p]),
+}
+
+
+def build(jobs: int = 8) -> str:
+    """Compile csrc/ with nvcc for sm_100a; returns the library path."""
+    subprocess.run(["make", "-s", f"-j{jobs}", "-C", os.path.join(HERE, "csrc")], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library.  There is no fallback: a missing library is an error."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                               "(make -C additive-fft-reed-solomon_b200/csrc)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib

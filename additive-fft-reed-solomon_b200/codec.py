@@ -1,0 +1,188 @@
+"""Host-side mirror of the reference crate's codec API over the C ABI.
+
+`Codec(n, t)` stands for the reference's `Rs::<N, T>` / `Codec<G, B, K, N, T>`
+(rs/src/lib.rs:20-45, rs/src/codec.rs:10-27) with the same method names,
+argument meaning and results:
+
+* ``encode_systematic_sharded(message, parity, workspace, shard_len)``
+  (codec.rs:241-265) XOR-accumulates into ``parity`` and transforms it, as the
+  reference does; ``workspace`` is accepted and not used.
+* ``recover_erasure_shards(received, workspace, shard_len, erasure_positions)``
+  (codec.rs:479-569) returns ``False`` iff there are more erasures than t and
+  otherwise rewrites the erased shards of ``received`` and returns ``True``.
+* ``recompute_data_from_parity_sharded(received, workspace, shard_len)``
+  (codec.rs:321-340, n == 2t).
+
+Buffers are numpy uint8 arrays in host memory (the call copies them to and
+from the GPU) or uint8 CUDA tensors (the call enqueues on the current torch
+stream and returns without waiting).  Where the reference panics (bad sizes,
+``unreachable!``), these raise ``AfrsError``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["AfrsError", "Context", "Codec", "fft_sharded", "ifft_sharded", "scale"]
+
+
+class AfrsError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        msg = _lib.lib().afrs_last_error().decode(errors="replace")
+        super().__init__(f"{where} failed ({code}): {msg}")
+        self.code = code
+
+
+def _check(code: int, where: str) -> int:
+    if code < 0:
+        raise AfrsError(code, where)
+    return code
+
+
+class Context:
+    """A device context (device tables, stream, scratch for host buffers)."""
+
+    _by_device: dict = {}
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        _check(_lib.lib().afrs_ctx_create(device, ctypes.byref(self._h)), "afrs_ctx_create")
+        self.device = device
+
+    @classmethod
+    def get(cls, device: int = 0) -> "Context":
+        ctx = cls._by_device.get(device)
+        if ctx is None:
+            ctx = cls._by_device[device] = cls(device)
+        return ctx
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().afrs_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _is_cuda_tensor(x) -> bool:
+    return hasattr(x, "is_cuda") and x.is_cuda
+
+
+def _dev_ptr(x) -> int:
+    import torch
+
+    if x.dtype != torch.uint8 or not x.is_contiguous():
+        raise AfrsError(_lib.AFRS_EINVAL, "tensor must be contiguous uint8")
+    return x.data_ptr()
+
+
+def _host_ptr(x: np.ndarray) -> int:
+    if not isinstance(x, np.ndarray) or x.dtype != np.uint8 or not x.flags["C_CONTIGUOUS"]:
+        raise AfrsError(_lib.AFRS_EINVAL, "host buffer must be a C-contiguous numpy uint8 array")
+    return x.ctypes.data
+
+
+def _stream(x) -> int:
+    import torch
+
+    return torch.cuda.current_stream(x.device).cuda_stream
+
+
+def _nbytes(x) -> int:
+    return x.numel() if _is_cuda_tensor(x) else x.size
+
+
+class Codec:
+    """Mirror of ``Rs::<N, T>`` (rs/src/lib.rs:20-45) running on the GPU."""
+
+    def __init__(self, n: int, t: int, device: int = 0):
+        self.n, self.t = int(n), int(t)
+        self.ctx = Context.get(device)
+
+    def _sizes(self, shard_len: int, **bufs) -> None:
+        want = {"message": (self.n - self.t) * shard_len, "parity": self.t * shard_len,
+                "received": self.n * shard_len}
+        for name, buf in bufs.items():
+            if _nbytes(buf) != want[name]:
+                raise AfrsError(_lib.AFRS_EINVAL, f"{name} has {_nbytes(buf)} bytes, expected {want[name]}")
+
+    def encode_systematic_sharded(self, message, parity, workspace=None, shard_len: int = 0) -> None:
+        self._sizes(shard_len, message=message, parity=parity)
+        L = _lib.lib()
+        if _is_cuda_tensor(message):
+            _check(L.afrs_encode_dev(self.ctx.handle, self.n, self.t, _dev_ptr(message), _dev_ptr(parity),
+                                     shard_len, 1, _stream(message)), "afrs_encode_dev")
+        else:
+            _check(L.afrs_encode(self.ctx.handle, self.n, self.t, _host_ptr(message), _host_ptr(parity),
+                                 shard_len, 1), "afrs_encode")
+
+    def encode_parity(self, message, parity, shard_len: int) -> None:
+        """Encode into ``parity`` without reading it (parity treated as zero)."""
+        self._sizes(shard_len, message=message, parity=parity)
+        L = _lib.lib()
+        if _is_cuda_tensor(message):
+            _check(L.afrs_encode_dev(self.ctx.handle, self.n, self.t, _dev_ptr(message), _dev_ptr(parity),
+                                     shard_len, 0, _stream(message)), "afrs_encode_dev")
+        else:
+            _check(L.afrs_encode(self.ctx.handle, self.n, self.t, _host_ptr(message), _host_ptr(parity),
+                                 shard_len, 0), "afrs_encode")
+
+    def recover_erasure_shards(self, received, workspace=None, shard_len: int = 0, erasure_positions=()) -> bool:
+        self._sizes(shard_len, received=received)
+        pos = np.ascontiguousarray(np.asarray(list(erasure_positions), dtype=np.int64))
+        if pos.size and (pos.min() < 0 or pos.max() > 255):
+            raise AfrsError(_lib.AFRS_EINVAL, "erasure positions must fit in u8")
+        pos8 = pos.astype(np.uint8)
+        pp = pos8.ctypes.data if pos8.size else None
+        L = _lib.lib()
+        if _is_cuda_tensor(received):
+            r = L.afrs_recover_dev(self.ctx.handle, self.n, self.t, _dev_ptr(received), shard_len, pp, pos8.size,
+                                   _stream(received))
+        else:
+            r = L.afrs_recover(self.ctx.handle, self.n, self.t, _host_ptr(received), shard_len, pp, pos8.size)
+        return bool(_check(r, "recover_erasure_shards"))
+
+    def recompute_data_from_parity_sharded(self, received, workspace=None, shard_len: int = 0) -> None:
+        self._sizes(shard_len, received=received)
+        if not _is_cuda_tensor(received):
+            import torch
+
+            d = torch.from_numpy(received).cuda(self.ctx.device)
+            self.recompute_data_from_parity_sharded(d, None, shard_len)
+            received[...] = d.cpu().numpy()
+            return
+        _check(_lib.lib().afrs_recompute_data_from_parity_dev(self.ctx.handle, self.n, self.t, _dev_ptr(received),
+                                                              shard_len, _stream(received)),
+               "recompute_data_from_parity")
+
+
+def fft_sharded(shards, shard_len: int, k: int, beta: int, device: int = 0) -> None:
+    """Kernel::fft_sharded (rs/src/kernel/mod.rs:8-14) on a uint8 CUDA tensor."""
+    ctx = Context.get(device)
+    _check(_lib.lib().afrs_fft_sharded_dev(ctx.handle, _dev_ptr(shards), shard_len, k, beta, _stream(shards)),
+           "fft_sharded")
+
+
+def ifft_sharded(shards, shard_len: int, k: int, beta: int, device: int = 0) -> None:
+    """Kernel::ifft_sharded (rs/src/kernel/mod.rs:15-21) on a uint8 CUDA tensor."""
+    ctx = Context.get(device)
+    _check(_lib.lib().afrs_ifft_sharded_dev(ctx.handle, _dev_ptr(shards), shard_len, k, beta, _stream(shards)),
+           "ifft_sharded")
+
+
+def scale(src, dst, scalar: int, device: int = 0) -> None:
+    """Kernel::scale (rs/src/kernel/mod.rs:22): dst = scalar * src, bytewise."""
+    ctx = Context.get(device)
+    _check(_lib.lib().afrs_scale_dev(ctx.handle, _dev_ptr(src), _dev_ptr(dst), src.numel(), scalar, _stream(src)),
+           "scale")

@@ -1,0 +1,268 @@
+// C ABI of libafrs_b200.so (declared in include/afrs.h).
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/afrs.h"
+#include "afrs_internal.h"
+
+struct afrs_ctx {
+  int device;
+  cudaStream_t stream;
+  uint8_t* scratch;  // device arena for the host-buffer entry points
+  size_t scratch_bytes;
+  std::mutex mu;
+};
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? AFRS_ENOMEM : AFRS_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+bool pow2(uint32_t v) { return v && !(v & (v - 1)); }
+
+int check_nt(uint32_t n, uint32_t t) {
+  if (!pow2(n) || n > 256 || n < 2) return fail(AFRS_EINVAL, "n=%u must be a power of two in [2, 256]", n);
+  if (!pow2(t) || t >= n) return fail(AFRS_EINVAL, "t=%u must be a power of two below n=%u", t, n);
+  return AFRS_OK;
+}
+
+// Positions must be distinct and < n; the reference leaves this unchecked
+// (a duplicate gives a zero denominator there, codec.rs:457-462).
+int check_positions(uint32_t n, const uint8_t* pos, size_t e) {
+  if (e && !pos) return fail(AFRS_EINVAL, "positions is NULL with e=%zu", e);
+  bool seen[256] = {};
+  for (size_t i = 0; i < e; i++) {
+    if (pos[i] >= n) return fail(AFRS_EINVAL, "erasure position %u >= n=%u", pos[i], n);
+    if (seen[pos[i]]) return fail(AFRS_EINVAL, "duplicate erasure position %u", pos[i]);
+    seen[pos[i]] = true;
+  }
+  return AFRS_OK;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+cudaError_t ensure_scratch(afrs_ctx* c, size_t bytes) {
+  if (bytes <= c->scratch_bytes) return cudaSuccess;
+  if (c->scratch) cudaFree(c->scratch);
+  c->scratch = nullptr;
+  c->scratch_bytes = 0;
+  cudaError_t e = cudaMalloc(&c->scratch, bytes);
+  if (e == cudaSuccess) c->scratch_bytes = bytes;
+  return e;
+}
+
+int launch_encode(const afrs::EncodeArgs& a, cudaStream_t s) {
+  cudaError_t e = afrs::launch_encode_special(a, s);
+  if (e == cudaErrorNotSupported) e = afrs::launch_encode_generic(a, s);
+  return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "encode launch");
+}
+
+int launch_recover(const afrs::RecoverArgs& a, cudaStream_t s) {
+  cudaError_t e = afrs::launch_recover_special(a, s);
+  if (e == cudaErrorNotSupported) e = afrs::launch_recover_generic(a, s);
+  return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "recover launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* afrs_last_error(void) { return g_err; }
+
+const char* afrs_version(void) { return "afrs_b200 0.1 sm_100a (bit-sliced GF(2^8) additive FFT)"; }
+
+int afrs_ctx_create(int device, afrs_ctx** out) {
+  if (!out) return fail(AFRS_EINVAL, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= count) return fail(AFRS_EINVAL, "device %d out of range (%d devices)", device, count);
+  DeviceGuard g(device);
+  afrs_ctx* c = new (std::nothrow) afrs_ctx;
+  if (!c) return fail(AFRS_ENOMEM, "context allocation");
+  c->device = device;
+  c->scratch = nullptr;
+  c->scratch_bytes = 0;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  *out = c;
+  return AFRS_OK;
+}
+
+void afrs_ctx_destroy(afrs_ctx* c) {
+  if (!c) return;
+  DeviceGuard g(c->device);
+  cudaStreamSynchronize(c->stream);
+  if (c->scratch) cudaFree(c->scratch);
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int afrs_encode_dev(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* d_message, uint8_t* d_parity,
+                    size_t L, int accumulate, void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  int r = check_nt(n, t);
+  if (r) return r;
+  if (L == 0) return AFRS_OK;
+  if (!d_message || !d_parity) return fail(AFRS_EINVAL, "NULL buffer");
+  DeviceGuard g(c->device);
+  afrs::EncodeArgs a{d_message, d_parity, L, (int)n, (int)t, accumulate ? 1 : 0};
+  return launch_encode(a, static_cast<cudaStream_t>(stream));
+}
+
+int afrs_recover_dev(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* d_received, size_t L,
+                     const uint8_t* positions, size_t e, void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  int r = check_nt(n, t);
+  if (r) return r;
+  if (e > t) return 0;
+  if (e == 0) return 1;
+  r = check_positions(n, positions, e);
+  if (r) return r;
+  if (L == 0) return 1;
+  if (!d_received) return fail(AFRS_EINVAL, "NULL buffer");
+  DeviceGuard g(c->device);
+  afrs::RecoverArgs a{};
+  a.rx = d_received;
+  a.L = L;
+  a.n = (int)n;
+  a.t = (int)t;
+  a.e = (int)e;
+  std::memcpy(a.pos, positions, e);
+  r = launch_recover(a, static_cast<cudaStream_t>(stream));
+  return r ? r : 1;
+}
+
+int afrs_encode(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* message, uint8_t* parity, size_t L,
+                int accumulate) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  int r = check_nt(n, t);
+  if (r) return r;
+  if (L == 0) return AFRS_OK;
+  if (!message || !parity) return fail(AFRS_EINVAL, "NULL buffer");
+  std::lock_guard<std::mutex> lk(c->mu);
+  DeviceGuard g(c->device);
+  const size_t mb = (size_t)(n - t) * L, pb = (size_t)t * L;
+  cudaError_t e = ensure_scratch(c, mb + pb);
+  if (e != cudaSuccess) return cuda_fail(e, "scratch allocation");
+  uint8_t* dm = c->scratch;
+  uint8_t* dp = c->scratch + mb;
+  if ((e = cudaMemcpyAsync(dm, message, mb, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "H2D message");
+  if (accumulate && (e = cudaMemcpyAsync(dp, parity, pb, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "H2D parity");
+  afrs::EncodeArgs a{dm, dp, L, (int)n, (int)t, accumulate ? 1 : 0};
+  if ((r = launch_encode(a, c->stream))) return r;
+  if ((e = cudaMemcpyAsync(parity, dp, pb, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "D2H parity");
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "encode");
+  return AFRS_OK;
+}
+
+int afrs_recover(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* received, size_t L, const uint8_t* positions,
+                 size_t e_count) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  int r = check_nt(n, t);
+  if (r) return r;
+  if (e_count > t) return 0;
+  if (e_count == 0) return 1;
+  r = check_positions(n, positions, e_count);
+  if (r) return r;
+  if (L == 0) return 1;
+  if (!received) return fail(AFRS_EINVAL, "NULL buffer");
+  std::lock_guard<std::mutex> lk(c->mu);
+  DeviceGuard g(c->device);
+  const size_t bytes = (size_t)n * L;
+  cudaError_t e = ensure_scratch(c, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "scratch allocation");
+  if ((e = cudaMemcpyAsync(c->scratch, received, bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "H2D received");
+  afrs::RecoverArgs a{};
+  a.rx = c->scratch;
+  a.L = L;
+  a.n = (int)n;
+  a.t = (int)t;
+  a.e = (int)e_count;
+  std::memcpy(a.pos, positions, e_count);
+  if ((r = launch_recover(a, c->stream))) return r;
+  // Only the erased shards change: copy just those back.
+  for (size_t j = 0; j < e_count; j++) {
+    const size_t off = (size_t)positions[j] * L;
+    if ((e = cudaMemcpyAsync(received + off, c->scratch + off, L, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
+      return cuda_fail(e, "D2H recovered shard");
+  }
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "recover");
+  return 1;
+}
+
+int afrs_recompute_data_from_parity_dev(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* d_received, size_t L,
+                                        void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  int r = check_nt(n, t);
+  if (r) return r;
+  if (n != 2 * t) return fail(AFRS_EINVAL, "recompute needs n == 2t (n=%u, t=%u)", n, t);
+  if (L == 0) return AFRS_OK;
+  if (!d_received) return fail(AFRS_EINVAL, "NULL buffer");
+  DeviceGuard g(c->device);
+  cudaError_t e = afrs::launch_recompute_generic(d_received, L, (int)t, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "recompute launch");
+}
+
+static int transform_dev(afrs_ctx* c, uint8_t* d, size_t L, uint32_t k, uint8_t beta, bool inverse, void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (k > 8) return fail(AFRS_EINVAL, "k=%u must be in 0..=8", k);
+  if (L == 0) return AFRS_OK;
+  if (!d) return fail(AFRS_EINVAL, "NULL buffer");
+  DeviceGuard g(c->device);
+  cudaError_t e = afrs::launch_transform_generic(d, L, (int)k, beta, inverse, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "transform launch");
+}
+
+int afrs_fft_sharded_dev(afrs_ctx* c, uint8_t* d, size_t L, uint32_t k, uint8_t beta, void* stream) {
+  return transform_dev(c, d, L, k, beta, false, stream);
+}
+
+int afrs_ifft_sharded_dev(afrs_ctx* c, uint8_t* d, size_t L, uint32_t k, uint8_t beta, void* stream) {
+  return transform_dev(c, d, L, k, beta, true, stream);
+}
+
+int afrs_scale_dev(afrs_ctx* c, const uint8_t* src, uint8_t* dst, size_t len, uint8_t scalar, void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (len == 0) return AFRS_OK;
+  if (!src || !dst) return fail(AFRS_EINVAL, "NULL buffer");
+  DeviceGuard g(c->device);
+  cudaError_t e = afrs::launch_scale(src, dst, len, scalar, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "scale launch");
+}
+
+}  // extern "C"

@@ -1,0 +1,41 @@
+// Internal interfaces between the C ABI (afrs_capi.cu) and the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace afrs {
+
+// Parameters of one recover launch, passed by value (kernel parameter space),
+// so a launch needs no device allocation.
+struct RecoverArgs {
+  uint8_t* rx;       // n * L bytes, shard-major
+  size_t L;          // shard length
+  int n, t, e;       // shards, parity shards, erasures
+  uint8_t pos[256];  // erased positions (first e entries)
+};
+
+struct EncodeArgs {
+  const uint8_t* msg;  // (n - t) * L
+  uint8_t* parity;     // t * L
+  size_t L;
+  int n, t;
+  int accumulate;
+};
+
+// Generic kernels: any (n, t), runtime twiddles.
+cudaError_t launch_encode_generic(const EncodeArgs& a, cudaStream_t s);
+cudaError_t launch_recover_generic(const RecoverArgs& a, cudaStream_t s);
+cudaError_t launch_transform_generic(uint8_t* shards, size_t L, int k, uint8_t beta, bool inverse,
+                                     cudaStream_t s);
+cudaError_t launch_recompute_generic(uint8_t* rx, size_t L, int t, cudaStream_t s);
+cudaError_t launch_scale(const uint8_t* src, uint8_t* dst, size_t len, uint8_t c, cudaStream_t s);
+
+// Specialised kernels (compile-time twiddles).  Return cudaErrorNotSupported
+// when no specialisation exists for the shape; the caller then uses the
+// generic kernel.
+cudaError_t launch_encode_special(const EncodeArgs& a, cudaStream_t s);
+cudaError_t launch_recover_special(const RecoverArgs& a, cudaStream_t s);
+
+}  // namespace afrs

@@ -1,0 +1,308 @@
+"""Benchmark: sharded RS encode + 128-erasure recover, n=256, k=128, 64 KiB
+shards (the reference's bandwidth case), on B200.
+
+One step = encode of one codeword (k*L read, t*L written) + recover of t
+uniformly random erasures of one codeword ((n-t)*L read, t*L written); the
+metric counts n*L bytes per operation (shards read + shards written).
+Inputs rotate over enough codewords that every step reads data that is not
+in L2.  Prints one JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's CPU algorithm instead: the reference
+is a Rust crate and no Rust toolchain exists here, so its GFNI kernel
+(rs/src/kernel/gfni_kernel.rs) and codec sequence (rs/src/codec.rs) are timed
+as their C restatement in oracle/gfni_baseline.c, on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SHARDS, T_PARITY, SHARD_LEN = 256, 128, 65536
+METRIC = "encode & recover GB/s (% of HBM peak)"
+WORKLOAD = "n=256 k=128 t=128, 64 KiB shards: encode + recover of 128 random erasures (one codeword each)"
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(seconds: float, threads: int):
+    """GFNI restatement of the reference's kernel + codec on host cores, on a
+    bounded sample of the same workload (same n, t, L)."""
+    from oracle import oracle
+
+    n, t, L = N_SHARDS, T_PARITY, SHARD_LEN
+    probe_e = oracle.gfni_throughput("encode", n, t, L, 1, 1)
+    probe_r = oracle.gfni_throughput("recover", n, t, L, 1, 1)
+    per_pair = n * L / probe_e + n * L / probe_r  # seconds for one encode + one recover, one thread
+    iters = max(1, int(seconds / max(per_pair, 1e-6) / 2))
+    enc = oracle.gfni_throughput("encode", n, t, L, iters, threads, 42)
+    rec = oracle.gfni_throughput("recover", n, t, L, iters, threads, 43)
+    combined = 2.0 / (1.0 / enc + 1.0 / rec)  # same mix as one GPU step: one encode + one recover
+    sample = f"{iters} encodes + {iters} recovers of one n=256 t=128 L=64KiB codeword per thread, {threads} threads"
+    return combined / 1e9, enc / 1e9, rec / 1e9, sample
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    vals = []
+    enc = rec = 0.0
+    sample = ""
+    for _ in range(args.warmup):
+        cpu_baseline(0.5, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, enc, rec, sample = cpu_baseline(2.0, threads)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = statistics.median(vals)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * wall / max(args.steps, 1), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": N_SHARDS, "k": N_SHARDS - T_PARITY, "t": T_PARITY,
+                   "shard_len": SHARD_LEN, "erasures": T_PARITY},
+        "encode_gbs": round(enc, 3), "recover_gbs": round(rec, 3),
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": sample + " (C restatement of rs/src/kernel/gfni_kernel.rs; no Rust toolchain)"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="afrs", choices=["afrs", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import __graft_entry__
+
+    afrs = __graft_entry__.load_package()
+    from oracle import oracle
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    n, t, L = N_SHARDS, T_PARITY, SHARD_LEN
+    k = n - t
+    op_bytes = n * L
+    # 16 codewords per role: 16 * (16 MiB encode + 16 MiB recover) = 512 MiB > L2.
+    R = 16
+    rng = np.random.default_rng(1234 + rank)
+    msg0 = oracle.random_bytes(k * L, 42 + rank)
+    par0 = np.zeros(t * L, np.uint8)
+    oracle.encode_systematic_sharded(n, t, msg0, par0, L)
+    cw0 = np.concatenate([par0, msg0])
+    enc_bufs, rec_bufs, patterns = [], [], []
+    dev = torch.device("cuda", local)
+    for r in range(R):
+        m = torch.from_numpy(oracle.random_bytes(k * L, 1000 + r) if r else msg0).to(dev)
+        enc_bufs.append((m, torch.zeros(t * L, dtype=torch.uint8, device=dev)))
+        pos = sorted(rng.choice(n, t, replace=False).tolist())
+        rx = cw0.copy()
+        for p in pos:
+            rx[p * L:(p + 1) * L] = 0
+        rec_bufs.append(torch.from_numpy(rx).to(dev))
+        patterns.append(pos)
+    codec = afrs.Codec(n, t, device=local)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(i, ev=None):
+        m, p = enc_bufs[i % R]
+        if ev is not None:
+            ev[0].record(stream)
+        codec.encode_parity(m, p, L)
+        if ev is not None:
+            ev[1].record(stream)
+        ok = codec.recover_erasure_shards(rec_bufs[i % R], None, L, patterns[i % R])
+        if ev is not None:
+            ev[2].record(stream)
+        return ok
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    # correctness of the measured path on codeword 0
+    assert (enc_bufs[0][1].cpu().numpy() == par0).all(), "encode mismatch vs oracle"
+    assert (rec_bufs[0].cpu().numpy() == cw0).all(), "recover mismatch vs oracle"
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for i in range(args.steps):
+        step(args.warmup + i, evs[i])
+    end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    elapsed_ms = start.elapsed_time(end)
+    enc_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    rec_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    if world > 1:
+        tt = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tt.item())
+
+    ms_per_step = elapsed_ms / args.steps
+    value = world * 2 * op_bytes / (ms_per_step * 1e-3) / 1e9
+    enc_avg, rec_avg = statistics.mean(enc_ms), statistics.mean(rec_ms)
+    peak, peak_kind = measured_peak_gbs()
+    dom = "recover" if rec_avg >= enc_avg else "encode"
+    dom_ms = max(enc_avg, rec_avg)
+    achieved = op_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = profile_traffic().get(dom)
+
+    # End to end through the public host-buffer API (pinned host memory):
+    # every step copies the inputs in and the results out.
+    h_msg = torch.from_numpy(msg0).pin_memory().numpy()
+    h_par = torch.zeros(t * L, dtype=torch.uint8).pin_memory().numpy()
+    h_rx_src = torch.from_numpy(rec_bufs[0].cpu().numpy()).pin_memory().numpy()
+    h_rx = torch.zeros(n * L, dtype=torch.uint8).pin_memory().numpy()
+    pos0 = patterns[0]
+    for p in pos0:
+        h_rx_src[p * L:(p + 1) * L] = 0
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        codec.encode_parity(h_msg, h_par, L)
+        h_rx[:] = h_rx_src
+        codec.recover_erasure_shards(h_rx, None, L, pos0)
+    assert (h_par == par0).all() and (h_rx == cw0).all(), "host-API result mismatch"
+    e2e_time = 0.0
+    for _ in range(e2e_steps):
+        h_rx[:] = h_rx_src  # host-side reset of the erased shards, not timed
+        t0 = time.perf_counter()
+        codec.encode_parity(h_msg, h_par, L)
+        codec.recover_erasure_shards(h_rx, None, L, pos0)
+        e2e_time += time.perf_counter() - t0
+    e2e_value = world * 2 * op_bytes * e2e_steps / e2e_time / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, ce, cr, sample = cpu_baseline(args.cpu_seconds, threads)
+        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample,
+               "encode_gbs": round(ce, 3), "recover_gbs": round(cr, 3)}
+
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "k": k, "t": t, "shard_len": L, "erasures": t,
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": f"inputs rotate over {R} encode + {R} recover codewords (512 MiB > 126 MB L2)"},
+        "encode_gbs": round(op_bytes / (enc_avg * 1e-3) / 1e9, 2),
+        "recover_gbs": round(op_bytes / (rec_avg * 1e-3) / 1e9, 2),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes": op_bytes},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "e2e": {"value": round(e2e_value, 3), "unit": "GB/s",
+                "h2d_bytes_per_step": k * L + n * L, "d2h_bytes_per_step": t * L + t * L},
+        "gpu_launches": 2 * args.steps,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,96 @@
+/*
+ * afrs.h - C ABI of the B200 (sm_100a) sharded additive-FFT Reed-Solomon
+ * library, libafrs_b200.so.
+ *
+ * Drop-in boundary for the hot path of vkomenda/additive-fft-reed-solomon:
+ * the sharded systematic encoder and the sharded erasure decoder over
+ * GF(2^8) (poly 0x11d, Cantor-basis evaluation points).  Every entry point
+ * takes plain pointers and sizes; results are bit-identical to the
+ * reference on the same inputs.
+ *
+ * Layout (as in the reference): a codeword is n shards of shard_len bytes,
+ * shard-major; shards 0..t-1 are parity, t..n-1 are message
+ * (rs/src/codec.rs:504-523).  n and t are powers of two, 1 <= t < n <= 256
+ * (rs/src/lib.rs:15-19).
+ *
+ * Return codes: AFRS_OK (0) or a negative AFRS_E* code.  The recover entry
+ * points return 1 for the reference's `true`, 0 for its `false` (more
+ * erasures than t), negative on error.  afrs_last_error() gives a message
+ * for the calling thread's last error.
+ */
+#ifndef AFRS_H
+#define AFRS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AFRS_OK 0
+#define AFRS_EINVAL (-1)   /* bad n, t, shard length, or erasure positions */
+#define AFRS_ECUDA (-2)    /* a CUDA call failed */
+#define AFRS_ENOMEM (-3)   /* device or pinned allocation failed */
+#define AFRS_ETIMEOUT (-4) /* a bounded device wait gave up */
+
+typedef struct afrs_ctx afrs_ctx;
+
+/* Context: device tables, a scratch arena for the host-buffer entry points
+ * and a stream.  The reference's Codec is a zero-sized value
+ * (rs/src/codec.rs:10-27, Codec::new :22-27); the context is its device-side
+ * counterpart.  One context may be used from one thread at a time. */
+int afrs_ctx_create(int device, afrs_ctx** out);
+void afrs_ctx_destroy(afrs_ctx* ctx);
+const char* afrs_last_error(void);
+
+/* Replaces Codec::encode_systematic_sharded (rs/src/codec.rs:241-265) on
+ * host buffers: message = (n-t)*shard_len bytes, parity = t*shard_len bytes.
+ * accumulate != 0 reproduces the reference exactly: the result is
+ * FFT_t(parity_in ^ sum of chunk IFFTs), i.e. the parity buffer is
+ * XOR-accumulated as the reference does; accumulate == 0 treats parity_in as
+ * zero, which is what every reference caller passes (encode bench:87,
+ * rs/src/poly_11d_lut.rs:106).  Synchronous. */
+int afrs_encode(afrs_ctx* ctx, uint32_t n, uint32_t t, const uint8_t* message, uint8_t* parity,
+                size_t shard_len, int accumulate);
+
+/* Replaces Codec::recover_erasure_shards (rs/src/codec.rs:479-569) on a
+ * host buffer of n*shard_len bytes.  Rewrites only the erased shards.
+ * Precondition (as in the reference, recover bench:128-132): the erased
+ * shards are zero on entry; the decoder does not read them.  positions must
+ * be distinct and < n (the reference does not check; here AFRS_EINVAL).
+ * Returns 1 (recovered), 0 (e > t, nothing written), or < 0.  Synchronous. */
+int afrs_recover(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* received, size_t shard_len,
+                 const uint8_t* positions, size_t e);
+
+/* Device-pointer variants of the two calls above, enqueued on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream).  Positions are read
+ * from host memory during the call.  They allocate nothing. */
+int afrs_encode_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, const uint8_t* d_message,
+                    uint8_t* d_parity, size_t shard_len, int accumulate, void* stream);
+int afrs_recover_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* d_received,
+                     size_t shard_len, const uint8_t* positions, size_t e, void* stream);
+
+/* Replaces Codec::recompute_data_from_parity_sharded (rs/src/codec.rs:321-340),
+ * n == 2t: rewrites the t message shards of d_received from its t parity
+ * shards. */
+int afrs_recompute_data_from_parity_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* d_received,
+                                        size_t shard_len, void* stream);
+
+/* The Kernel trait (rs/src/kernel/mod.rs:7-24) on device buffers:
+ * fft_sharded / ifft_sharded over 2^k shards at coset beta, in place, and
+ * scale (dst = scalar * src, dst may equal src). */
+int afrs_fft_sharded_dev(afrs_ctx* ctx, uint8_t* d_shards, size_t shard_len, uint32_t k, uint8_t beta,
+                         void* stream);
+int afrs_ifft_sharded_dev(afrs_ctx* ctx, uint8_t* d_shards, size_t shard_len, uint32_t k, uint8_t beta,
+                          void* stream);
+int afrs_scale_dev(afrs_ctx* ctx, const uint8_t* d_src, uint8_t* d_dst, size_t len, uint8_t scalar,
+                   void* stream);
+
+/* Library build information (kernel set, arch) for logs. */
+const char* afrs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFRS_H */

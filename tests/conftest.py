@@ -28,3 +28,10 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if "gpu" in item.keywords:
             item.add_marker(skip)
+
+
+@pytest.fixture(scope="session")
+def afrs():
+    import __graft_entry__
+
+    return __graft_entry__.load_package()

@@ -1,0 +1,203 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle,
+bit-exact, on seeded inputs.  Covers every (n, t) shape the reference's own
+tests cover (rs/src/poly_11d_lut.rs:431-566), odd and misaligned shard
+lengths, random and adversarial erasure patterns, and the Kernel-trait ops."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+torch = pytest.importorskip("torch")
+
+PAIRS_ALL = [(n, t) for n in (2, 4, 8, 16, 32, 64, 128, 256) for t in (1, 2, 4, 8, 16, 32, 64, 128) if t < n]
+T = oracle.tables()
+
+
+def _codeword(n, t, L, seed):
+    msg = oracle.random_bytes((n - t) * L, seed)
+    par = np.zeros(t * L, np.uint8)
+    oracle.encode_systematic_sharded(n, t, msg, par, L)
+    return msg, par
+
+
+def _erase(cw, L, pos):
+    rx = cw.copy()
+    for p in pos:
+        rx[p * L:(p + 1) * L] = 0
+    return rx
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t", PAIRS_ALL)
+@pytest.mark.parametrize("L", [1, 33, 256])
+def test_encode_matches_oracle(afrs, n, t, L):
+    msg, ref = _codeword(n, t, L, seed=n * 131 + t * 7 + L)
+    d_par = torch.zeros(t * L, dtype=torch.uint8, device="cuda")
+    afrs.Codec(n, t).encode_parity(torch.from_numpy(msg).cuda(), d_par, L)
+    assert (d_par.cpu().numpy() == ref).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t", [(4, 2), (32, 8), (64, 32), (256, 128), (256, 32), (128, 4)])
+def test_encode_accumulates_like_reference(afrs, n, t):
+    # codec.rs:259-264: parity buffer is XOR-accumulated before the final FFT.
+    L = 100
+    msg = oracle.random_bytes((n - t) * L, 3)
+    p0 = oracle.random_bytes(t * L, 4)
+    ref = p0.copy()
+    oracle.encode_systematic_sharded(n, t, msg, ref, L)
+    got = p0.copy()
+    afrs.Codec(n, t).encode_systematic_sharded(msg, got, None, L)  # host buffers
+    assert (got == ref).all()
+    d = torch.from_numpy(p0.copy()).cuda()
+    afrs.Codec(n, t).encode_systematic_sharded(torch.from_numpy(msg).cuda(), d, None, L)
+    assert (d.cpu().numpy() == ref).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t", PAIRS_ALL)
+def test_recover_reference_pattern(afrs, n, t):
+    # rs/src/poly_11d_lut.rs:536-566: L = 1, erase odd positions 1..2T-1,
+    # message[i][j] = T + i + j.
+    L = 1
+    msg = ((t + np.arange(n - t)) % 256).astype(np.uint8)
+    par = np.zeros(t, np.uint8)
+    oracle.encode_systematic_sharded(n, t, msg, par, L)
+    cw = np.concatenate([par, msg])
+    pos = list(range(1, 2 * t, 2))
+    d = torch.from_numpy(_erase(cw, L, pos)).cuda()
+    assert afrs.Codec(n, t).recover_erasure_shards(d, None, L, pos)
+    assert (d.cpu().numpy() == cw).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t", PAIRS_ALL)
+def test_recover_random_patterns_match_oracle(afrs, n, t):
+    rng = np.random.default_rng(n * 17 + t)
+    L = 77
+    msg, par = _codeword(n, t, L, seed=n + t)
+    cw = np.concatenate([par, msg])
+    codec = afrs.Codec(n, t)
+    for e in sorted({1, max(1, t // 2), t}):
+        pos = rng.choice(n, e, replace=False).tolist()
+        rx = _erase(cw, L, pos)
+        ref = rx.copy()
+        assert oracle.recover_erasure_shards(n, t, ref, L, pos)
+        d = torch.from_numpy(rx).cuda()
+        assert codec.recover_erasure_shards(d, None, L, pos)
+        out = d.cpu().numpy()
+        assert (out == ref).all() and (out == cw).all(), (n, t, e)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t", [(16, 8), (64, 16), (256, 64), (256, 128)])
+def test_recover_non_codeword_input_matches_reference(afrs, n, t):
+    # Surviving rows that are not a codeword (e < t): the GPU decoder still
+    # computes the reference's map exactly (erased rows zero).
+    rng = np.random.default_rng(99 + n + t)
+    L = 48
+    for e in sorted({1, t // 2}):
+        rx = rng.integers(0, 256, n * L, dtype=np.uint8)
+        pos = rng.choice(n, e, replace=False).tolist()
+        rx = _erase(rx, L, pos)
+        ref = rx.copy()
+        oracle.recover_erasure_shards(n, t, ref, L, pos)
+        d = torch.from_numpy(rx).cuda()
+        afrs.Codec(n, t).recover_erasure_shards(d, None, L, pos)
+        assert (d.cpu().numpy() == ref).all()
+
+
+@pytest.mark.gpu
+def test_host_buffer_api_and_adversarial_patterns(afrs):
+    n, t, L = 256, 32, 4096 + 3
+    msg, par = _codeword(n, t, L, seed=11)
+    cw = np.concatenate([par, msg])
+    codec = afrs.Codec(n, t)
+    got = np.zeros(t * L, np.uint8)
+    codec.encode_systematic_sharded(msg, got, None, L)
+    assert (got == par).all()
+    for pos in (list(range(40, 72)), list(range(200, 232)), list(range(0, 32)), list(range(224, 256))):
+        rx = _erase(cw, L, pos)
+        assert codec.recover_erasure_shards(rx, None, L, pos)
+        assert (rx == cw).all()
+
+
+@pytest.mark.gpu
+def test_misaligned_and_ragged_buffers(afrs):
+    n, t, L = 64, 16, 1000 + 1
+    msg, par = _codeword(n, t, L, seed=5)
+    cw = np.concatenate([par, msg])
+    big = torch.zeros(n * L + 64, dtype=torch.uint8, device="cuda")
+    for off in (1, 3, 8):
+        view = big[off:off + n * L]
+        view.copy_(torch.from_numpy(cw))
+        view[: t * L].zero_()
+        afrs.Codec(n, t).encode_parity(view[t * L:], view[: t * L], L)
+        assert (view.cpu().numpy() == cw).all()
+        pos = [0, 5, 17, 33, 40, 41, 62, 63]
+        for p in pos:
+            view[p * L:(p + 1) * L].zero_()
+        assert afrs.Codec(n, t).recover_erasure_shards(view, None, L, pos)
+        assert (view.cpu().numpy() == cw).all()
+
+
+@pytest.mark.gpu
+def test_recover_edge_cases(afrs):
+    n, t, L = 32, 8, 64
+    msg, par = _codeword(n, t, L, seed=2)
+    cw = np.concatenate([par, msg])
+    codec = afrs.Codec(n, t)
+    d = torch.from_numpy(cw.copy()).cuda()
+    assert codec.recover_erasure_shards(d, None, L, [])  # e == 0 -> true, no-op
+    assert not codec.recover_erasure_shards(d, None, L, list(range(9)))  # e > t -> false
+    assert (d.cpu().numpy() == cw).all()
+    with pytest.raises(afrs.AfrsError):
+        codec.recover_erasure_shards(d, None, L, [1, 1])
+    with pytest.raises(afrs.AfrsError):
+        codec.recover_erasure_shards(d, None, L, [40])
+    with pytest.raises(afrs.AfrsError):
+        afrs.Codec(24, 8)
+        afrs.Codec(24, 8).encode_parity(torch.zeros(16 * L, dtype=torch.uint8, device="cuda"),
+                                        torch.zeros(8 * L, dtype=torch.uint8, device="cuda"), L)
+    z = torch.zeros(0, dtype=torch.uint8, device="cuda")
+    afrs.Codec(4, 2).encode_parity(z, z, 0)  # empty shards
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L", [1, 63, 64, 65, 128, 1000])
+def test_kernel_trait_transforms_and_scale(afrs, L):
+    # rs/src/kernel/gfni_kernel.rs:324-387: input i*37 + j*13 + 1, beta = omega_n
+    for k in range(0, 9):
+        n = 1 << k
+        i = np.arange(n)[:, None]
+        j = np.arange(L)[None, :]
+        base = ((i * 37 + j * 13 + 1) % 256).astype(np.uint8).reshape(-1)
+        for beta in (0, int(T.subspace[n & 255]), 0x5A):
+            for inv in (False, True):
+                ref = base.copy()
+                (oracle.ifft_sharded if inv else oracle.fft_sharded)(ref, L, k, beta)
+                d = torch.from_numpy(base.copy()).cuda()
+                (afrs.ifft_sharded if inv else afrs.fft_sharded)(d, L, k, beta)
+                assert (d.cpu().numpy() == ref).all(), (k, beta, inv)
+    src = oracle.random_bytes(L, 1)
+    for c in (0, 1, 2, 0x53, 0xFF):
+        ref = np.zeros(L, np.uint8)
+        oracle.lib().orc_scale(src.ctypes.data_as(oracle._u8p), ref.ctypes.data_as(oracle._u8p), L, c)
+        d_src = torch.from_numpy(src).cuda()
+        d_dst = torch.empty_like(d_src)
+        afrs.scale(d_src, d_dst, c)
+        assert (d_dst.cpu().numpy() == ref).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("t", [1, 2, 8, 32, 128])
+def test_recompute_data_from_parity(afrs, t):
+    # rs/src/poly_11d_lut.rs:471-494
+    n, L = 2 * t, 16
+    msg, par = _codeword(n, t, L, seed=t)
+    cw = np.concatenate([par, msg])
+    rx = cw.copy()
+    rx[t * L:] = 0
+    d = torch.from_numpy(rx).cuda()
+    afrs.Codec(n, t).recompute_data_from_parity_sharded(d, None, L)
+    assert (d.cpu().numpy() == cw).all()
