@@ -1,0 +1,8 @@
+// Encode kernel for n = 8, t = 2.
+#include "special.cuh"
+
+namespace afrs {
+namespace spec {
+cudaError_t launch_enc_3_1(const EncodeArgs& a, cudaStream_t s) { return launch_enc<3, 1>(a, s); }
+}  // namespace spec
+}  // namespace afrs

@@ -1,0 +1,8 @@
+// Encode kernel for n = 256, t = 16.
+#include "special.cuh"
+
+namespace afrs {
+namespace spec {
+cudaError_t launch_enc_8_4(const EncodeArgs& a, cudaStream_t s) { return launch_enc<8, 4>(a, s); }
+}  // namespace spec
+}  // namespace afrs

@@ -1,0 +1,8 @@
+// Encode kernel for n = 256, t = 128.
+#include "special.cuh"
+
+namespace afrs {
+namespace spec {
+cudaError_t launch_enc_8_7(const EncodeArgs& a, cudaStream_t s) { return launch_enc<8, 7>(a, s); }
+}  // namespace spec
+}  // namespace afrs

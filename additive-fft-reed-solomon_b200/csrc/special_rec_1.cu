@@ -1,0 +1,8 @@
+// Recover kernel for n = 2.
+#include "special.cuh"
+
+namespace afrs {
+namespace spec {
+cudaError_t launch_rec_1(const RecoverArgs& a, cudaStream_t s) { return launch_rec<1>(a, s); }
+}  // namespace spec
+}  // namespace afrs

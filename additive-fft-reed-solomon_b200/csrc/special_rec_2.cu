@@ -1,0 +1,8 @@
+// Recover kernel for n = 4.
+#include "special.cuh"
+
+namespace afrs {
+namespace spec {
+cudaError_t launch_rec_2(const RecoverArgs& a, cudaStream_t s) { return launch_rec<2>(a, s); }
+}  // namespace spec
+}  // namespace afrs

@@ -1,0 +1,8 @@
+// Recover kernel for n = 16.
+#include "special.cuh"
+
+namespace afrs {
+namespace spec {
+cudaError_t launch_rec_4(const RecoverArgs& a, cudaStream_t s) { return launch_rec<4>(a, s); }
+}  // namespace spec
+}  // namespace afrs
