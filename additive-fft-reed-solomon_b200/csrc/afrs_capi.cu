@@ -12,9 +12,12 @@
 struct afrs_ctx {
   int device;
   cudaStream_t stream;
-  uint8_t* scratch;  // device arena for the host-buffer entry points
+  uint8_t* scratch;  // device staging for the host-buffer entry points
   size_t scratch_bytes;
-  std::mutex mu;
+  uint32_t* work;  // bit-sliced intermediate rows of the phase kernels
+  size_t work_bytes;
+  cudaEvent_t work_free;  // recorded after each use of `work`
+  std::recursive_mutex mu;
 };
 
 namespace {
@@ -77,15 +80,52 @@ cudaError_t ensure_scratch(afrs_ctx* c, size_t bytes) {
   return e;
 }
 
-int launch_encode(const afrs::EncodeArgs& a, cudaStream_t s) {
-  cudaError_t e = afrs::launch_encode_special(a, s);
+// Largest phase scratch a context keeps (the launchers batch columns beyond it).
+constexpr size_t kWorkCap = (size_t)48 << 20;
+
+// Grows the context's phase scratch to min(need, kWorkCap) and orders this
+// call after the previous user of the scratch (calls on different streams
+// would otherwise share it concurrently).
+cudaError_t acquire_work(afrs_ctx* c, size_t need, cudaStream_t s, afrs::ScratchArena* out) {
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  if (need > kWorkCap) need = kWorkCap;
+  if (need > c->work_bytes) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return e;
+    if (c->work) cudaFree(c->work);
+    c->work = nullptr;
+    c->work_bytes = 0;
+    e = cudaMalloc(reinterpret_cast<void**>(&c->work), need);
+    if (e != cudaSuccess) return e;
+    c->work_bytes = need;
+  }
+  cudaError_t e = cudaStreamWaitEvent(s, c->work_free, 0);
+  if (e != cudaSuccess) return e;
+  *out = afrs::ScratchArena{c->work, c->work_bytes};
+  return cudaSuccess;
+}
+
+cudaError_t release_work(afrs_ctx* c, cudaStream_t s) { return cudaEventRecord(c->work_free, s); }
+
+int launch_encode(afrs_ctx* c, const afrs::EncodeArgs& a, cudaStream_t s) {
+  afrs::ScratchArena sc{nullptr, 0};
+  cudaError_t e = cudaSuccess;
+  const size_t need = afrs::scratch_bytes_encode(a.n, a.t, a.L);
+  if (need && (e = acquire_work(c, need, s, &sc)) != cudaSuccess) return cuda_fail(e, "encode scratch");
+  e = afrs::launch_encode_special(a, sc, s);
   if (e == cudaErrorNotSupported) e = afrs::launch_encode_generic(a, s);
+  if (need && e == cudaSuccess) e = release_work(c, s);
   return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "encode launch");
 }
 
-int launch_recover(const afrs::RecoverArgs& a, cudaStream_t s) {
-  cudaError_t e = afrs::launch_recover_special(a, s);
+int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
+  afrs::ScratchArena sc{nullptr, 0};
+  cudaError_t e = cudaSuccess;
+  const size_t need = afrs::scratch_bytes_recover(a.n, a.L);
+  if (need && (e = acquire_work(c, need, s, &sc)) != cudaSuccess) return cuda_fail(e, "recover scratch");
+  e = afrs::launch_recover_special(a, sc, s);
   if (e == cudaErrorNotSupported) e = afrs::launch_recover_generic(a, s);
+  if (need && e == cudaSuccess) e = release_work(c, s);
   return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "recover launch");
 }
 
@@ -110,10 +150,18 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
   c->device = device;
   c->scratch = nullptr;
   c->scratch_bytes = 0;
+  c->work = nullptr;
+  c->work_bytes = 0;
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;
     return cuda_fail(e, "cudaStreamCreate");
+  }
+  e = cudaEventCreateWithFlags(&c->work_free, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return cuda_fail(e, "cudaEventCreate");
   }
   *out = c;
   return AFRS_OK;
@@ -122,8 +170,10 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
 void afrs_ctx_destroy(afrs_ctx* c) {
   if (!c) return;
   DeviceGuard g(c->device);
-  cudaStreamSynchronize(c->stream);
+  cudaDeviceSynchronize();
   if (c->scratch) cudaFree(c->scratch);
+  if (c->work) cudaFree(c->work);
+  cudaEventDestroy(c->work_free);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -137,7 +187,7 @@ int afrs_encode_dev(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* d_messag
   if (!d_message || !d_parity) return fail(AFRS_EINVAL, "NULL buffer");
   DeviceGuard g(c->device);
   afrs::EncodeArgs a{d_message, d_parity, L, (int)n, (int)t, accumulate ? 1 : 0};
-  return launch_encode(a, static_cast<cudaStream_t>(stream));
+  return launch_encode(c, a, static_cast<cudaStream_t>(stream));
 }
 
 int afrs_recover_dev(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* d_received, size_t L,
@@ -159,7 +209,7 @@ int afrs_recover_dev(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* d_received, s
   a.t = (int)t;
   a.e = (int)e;
   std::memcpy(a.pos, positions, e);
-  r = launch_recover(a, static_cast<cudaStream_t>(stream));
+  r = launch_recover(c, a, static_cast<cudaStream_t>(stream));
   return r ? r : 1;
 }
 
@@ -170,7 +220,7 @@ int afrs_encode(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* message, uin
   if (r) return r;
   if (L == 0) return AFRS_OK;
   if (!message || !parity) return fail(AFRS_EINVAL, "NULL buffer");
-  std::lock_guard<std::mutex> lk(c->mu);
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
   DeviceGuard g(c->device);
   const size_t mb = (size_t)(n - t) * L, pb = (size_t)t * L;
   cudaError_t e = ensure_scratch(c, mb + pb);
@@ -182,7 +232,7 @@ int afrs_encode(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* message, uin
   if (accumulate && (e = cudaMemcpyAsync(dp, parity, pb, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
     return cuda_fail(e, "H2D parity");
   afrs::EncodeArgs a{dm, dp, L, (int)n, (int)t, accumulate ? 1 : 0};
-  if ((r = launch_encode(a, c->stream))) return r;
+  if ((r = launch_encode(c, a, c->stream))) return r;
   if ((e = cudaMemcpyAsync(parity, dp, pb, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
     return cuda_fail(e, "D2H parity");
   if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "encode");
@@ -200,7 +250,7 @@ int afrs_recover(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* received, size_t 
   if (r) return r;
   if (L == 0) return 1;
   if (!received) return fail(AFRS_EINVAL, "NULL buffer");
-  std::lock_guard<std::mutex> lk(c->mu);
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
   DeviceGuard g(c->device);
   const size_t bytes = (size_t)n * L;
   cudaError_t e = ensure_scratch(c, bytes);
@@ -214,7 +264,7 @@ int afrs_recover(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* received, size_t 
   a.t = (int)t;
   a.e = (int)e_count;
   std::memcpy(a.pos, positions, e_count);
-  if ((r = launch_recover(a, c->stream))) return r;
+  if ((r = launch_recover(c, a, c->stream))) return r;
   // Only the erased shards change: copy just those back.
   for (size_t j = 0; j < e_count; j++) {
     const size_t off = (size_t)positions[j] * L;

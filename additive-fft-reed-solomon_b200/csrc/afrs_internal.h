@@ -32,10 +32,20 @@ cudaError_t launch_transform_generic(uint8_t* shards, size_t L, int k, uint8_t b
 cudaError_t launch_recompute_generic(uint8_t* rx, size_t L, int t, cudaStream_t s);
 cudaError_t launch_scale(const uint8_t* src, uint8_t* dst, size_t len, uint8_t c, cudaStream_t s);
 
+// Device scratch for the phase kernels (bit-sliced intermediate rows).
+struct ScratchArena {
+  uint32_t* ptr;  // 16-byte aligned
+  size_t bytes;
+};
+
 // Specialised kernels (compile-time twiddles).  Return cudaErrorNotSupported
 // when no specialisation exists for the shape; the caller then uses the
-// generic kernel.
-cudaError_t launch_encode_special(const EncodeArgs& a, cudaStream_t s);
-cudaError_t launch_recover_special(const RecoverArgs& a, cudaStream_t s);
+// generic kernel.  With less scratch than scratch_bytes_*() the launchers
+// process the shard in column batches; with none they need, they return
+// cudaErrorMemoryAllocation.
+cudaError_t launch_encode_special(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s);
+cudaError_t launch_recover_special(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s);
+size_t scratch_bytes_encode(int n, int t, size_t L);
+size_t scratch_bytes_recover(int n, size_t L);
 
 }  // namespace afrs

@@ -184,4 +184,47 @@ __host__ __device__ __forceinline__ void transpose8(uint32_t (&x)[8]) {
   }
 }
 
+// transpose8 with its shifts issued as integer multiplies, which execute on
+// the FMA pipe while the XOR/AND work occupies the ALU pipe (the bit-sliced
+// kernels are bound by the ALU pipe).  Left shifts by s are products by 2^s;
+// right shifts by s are the high words of products by 2^(32-s).  The factors
+// come from ShiftMul registers whose values the compiler cannot see, so it
+// keeps them as multiplies.
+struct ShiftMul {
+  uint32_t l1, l2, l4, r1, r2, r4;
+};
+
+__device__ __forceinline__ ShiftMul make_shift_mul() {
+  ShiftMul m;
+  asm("mov.u32 %0, 2;" : "=r"(m.l1));
+  asm("mov.u32 %0, 4;" : "=r"(m.l2));
+  asm("mov.u32 %0, 16;" : "=r"(m.l4));
+  asm("mov.u32 %0, 0x80000000;" : "=r"(m.r1));
+  asm("mov.u32 %0, 0x40000000;" : "=r"(m.r2));
+  asm("mov.u32 %0, 0x10000000;" : "=r"(m.r4));
+  return m;
+}
+
+__device__ __forceinline__ void transpose8f(uint32_t (&x)[8], const ShiftMul& k) {
+#pragma unroll
+  for (int w = 0; w < 4; w++) {
+    uint32_t t = (__umulhi(x[w], k.r4) ^ x[w + 4]) & 0x0F0F0F0Fu;
+    x[w + 4] ^= t;
+    x[w] ^= t * k.l4;
+  }
+#pragma unroll
+  for (int w = 0; w < 8; w++) {
+    if (w & 2) continue;
+    uint32_t t = (__umulhi(x[w], k.r2) ^ x[w + 2]) & 0x33333333u;
+    x[w + 2] ^= t;
+    x[w] ^= t * k.l2;
+  }
+#pragma unroll
+  for (int w = 0; w < 8; w += 2) {
+    uint32_t t = (__umulhi(x[w], k.r1) ^ x[w + 1]) & 0x55555555u;
+    x[w + 1] ^= t;
+    x[w] ^= t * k.l1;
+  }
+}
+
 }  // namespace afrs

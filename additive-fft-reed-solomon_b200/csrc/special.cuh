@@ -3,15 +3,21 @@
 //
 // Every twiddle of an additive FFT level depends only on the level, the
 // coset beta and the row bits above the level (rs/src/kernel/lut_kernel.rs:
-// 28-82), so once the thread's rows are fixed at compile time every
-// multiply is a fixed XOR network over bit-sliced planes (gf_device.cuh).
-// A warp owns 32 colwords (1024 byte-columns); rows are split between warps,
-// and a warp-uniform row group selects its compile-time variant.
+// 28-82), so once a thread's rows are fixed at compile time every multiply
+// is a fixed XOR network over bit-sliced planes (gf_device.cuh).
 //
-// Two-level schedule for 2^k rows, k >= 5 (radix 16 x 2^(k-4)):
-//   bottom pass: levels 0..3 on 16 contiguous rows (group g = row >> 4),
-//                one warp per group, variant chosen by g;
-//   top pass:    levels 4..k-1 on rows {b + 16 m}, uniform code for every b.
+// Transforms of 2^k rows, k >= 5, run as three phase kernels (radix 16 x
+// 2^(k-4)):
+//   bottom pass: levels 0..3 on 16 contiguous rows (group g = row >> 4);
+//   top pass:    levels 4..k-1 on rows {b + 16 m};
+//   bottom pass of the next transform.
+// The code of a bottom pass depends on g (its twiddles do), so each CTA runs
+// one g (blockIdx.y) over many columns: every fetched instruction is used by
+// all warps of the CTA.  (A single kernel holding all rows of a column tile
+// in shared memory runs each variant once per tile and is bound by
+// instruction fetch: ~800 KB of straight-line code for n = 256.)
+// Between phases the rows stay bit-sliced in a scratch buffer sized to stay
+// resident in L2; long shards are processed in column batches.
 // Transforms with k <= 4 run entirely inside one thread.
 #pragma once
 #include "afrs_internal.h"
@@ -122,13 +128,33 @@ __device__ __forceinline__ void sstore(uint32_t* sm, int row, int w, const uint3
   for (int p = 0; p < 8; p++) sm[(row * 8 + p) * CW + w] = x[p];
 }
 
-__device__ __forceinline__ void gload(const uint8_t* base, size_t row, size_t L, size_t col, uint32_t (&x)[8]) {
-  load32(base + row * L, col, L, x);
-  transpose8(x);
+// Shard row <-> bit-sliced planes for global colword w (io.cuh layout).
+__device__ __forceinline__ void gload(const uint8_t* base, size_t row, size_t L, size_t w, uint32_t (&x)[8],
+                                      const ShiftMul& km) {
+  load_cw(base + row * L, L, w, x);
+  transpose8f(x, km);
 }
-__device__ __forceinline__ void gstore(uint8_t* base, size_t row, size_t L, size_t col, uint32_t (&x)[8]) {
-  transpose8(x);
-  store32(base + row * L, col, L, x);
+__device__ __forceinline__ void gstore(uint8_t* base, size_t row, size_t L, size_t w, uint32_t (&x)[8],
+                                       const ShiftMul& km) {
+  transpose8f(x, km);
+  store_cw(base + row * L, L, w, x);
+}
+
+// y <- c * y for c = g^a (g = 2), a in [0, 254] uniform across the CTA:
+// a = 16 h + l and c = g^l * g^(16 h), two multiplies by compile-time
+// constants picked from 16 each (32 XOR networks of code in total).
+template <int C>
+__device__ __forceinline__ void mul_by_c(uint32_t (&y)[8]) {
+  if constexpr (C != 1) {
+    uint32_t r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    mul_xor_c<static_cast<uint8_t>(C)>(r, y);
+#pragma unroll
+    for (int p = 0; p < 8; p++) y[p] = r[p];
+  }
+}
+__device__ __forceinline__ void scale_log(uint32_t (&y)[8], int a) {
+  dispatch<0, 15>(a >> 4, [&](auto h) { mul_by_c<kField.exp[16 * decltype(h)::value]>(y); });
+  dispatch<0, 15>(a & 15, [&](auto l) { mul_by_c<kField.exp[decltype(l)::value]>(y); });
 }
 
 __device__ __forceinline__ void scale_rt(uint32_t (&x)[8], uint32_t c) {
@@ -157,7 +183,8 @@ __global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t slice = (size_t)blockIdx.x * (kThreads / 32) + warp;
   if (slice * 1024 >= a.L) return;
-  const size_t col = (slice * 32 + lane) * 32;
+  const size_t cw = slice * 32 + lane;
+  const ShiftMul km = make_shift_mul();
   uint32_t* wacc = sm + warp * (T * 8 * 32);  // per-warp accumulator when kSmemAcc
   uint32_t acc[kSmemAcc ? 1 : T][8];
   if constexpr (kSmemAcc) {
@@ -171,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
   for (int c = 1; c <= C; c++) {
     uint32_t x[T][8];
 #pragma unroll
-    for (int r = 0; r < T; r++) gload(a.msg, (size_t)(c - 1) * T + r, a.L, col, x[r]);
+    for (int r = 0; r < T; r++) gload(a.msg, (size_t)(c - 1) * T + r, a.L, cw, x[r], km);
     if constexpr (LOGT > 0) {
       dispatch<1, C>(c, [&](auto cc) {
         constexpr int CC = decltype(cc)::value;
@@ -204,128 +231,122 @@ __global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
       for (int p = 0; p < 8; p++) f[r][p] = acc[r][p];
     if (a.accumulate) {
       uint32_t y[8];
-      gload(a.parity, r, a.L, col, y);
+      gload(a.parity, r, a.L, cw, y, km);
 #pragma unroll
       for (int p = 0; p < 8; p++) f[r][p] ^= y[p];
     }
   }
   block_fft<0, LOGT, 0, 0, T>(f);
 #pragma unroll
-  for (int r = 0; r < T; r++) gstore(a.parity, r, a.L, col, f[r]);
+  for (int r = 0; r < T; r++) gstore(a.parity, r, a.L, cw, f[r], km);
 }
 
-// ---- encode, t >= 32: one CTA per 1024-column slice -----------------------
-// Chunks are processed in waves of 128/t (128 rows of shared memory):
-// bottom IFFT pass per (chunk, group) warp, then top IFFT pass accumulating
-// into registers; finally top FFT, bottom FFT and store.
-template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kThreads, 1) k_enc_large(EncodeArgs a) {
-  constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1;
-  constexpr int G = T / 16, WC = 128 / T, TL = LOGT - 4, TR = 1 << TL;
-  constexpr int WAVES = (C + WC - 1) / WC;
-  extern __shared__ uint32_t sm[];  // 128 rows x 8 planes x 32 colwords
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t col = ((size_t)blockIdx.x * 32 + lane) * 32;
 
-  uint32_t acc[WAVES > 1 ? 2 : 1][WAVES > 1 ? TR : 1][8];
-  if constexpr (WAVES > 1) {
+// ---- bit-sliced scratch ---------------------------------------------------
+// Row r, colword w of a batch of ncw colwords: planes 0..3 as one 16-byte
+// word at ((r * 2 + 0) * ncw + w) and planes 4..7 at ((r * 2 + 1) * ncw + w),
+// so that a warp over 32 consecutive colwords moves 512 contiguous bytes per
+// instruction.
+__device__ __forceinline__ void xload(const uint32_t* s, size_t ncw, int r, size_t w, uint32_t (&x)[8]) {
+  const uint4* q = reinterpret_cast<const uint4*>(s);
+  uint4 a = q[(size_t)(2 * r) * ncw + w], b = q[(size_t)(2 * r + 1) * ncw + w];
+  x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+  x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+__device__ __forceinline__ void xstore(uint32_t* s, size_t ncw, int r, size_t w, const uint32_t (&x)[8]) {
+  uint4* q = reinterpret_cast<uint4*>(s);
+  q[(size_t)(2 * r) * ncw + w] = make_uint4(x[0], x[1], x[2], x[3]);
+  q[(size_t)(2 * r + 1) * ncw + w] = make_uint4(x[4], x[5], x[6], x[7]);
+}
+
+// One batch of colwords [cw0, cw0 + ncw) of a phase kernel.
+struct Batch {
+  uint32_t* s1;  // scratch (bit-sliced rows)
+  uint32_t* s2;  // second scratch (recover)
+  size_t ncw;    // colwords in the batch
+  size_t cw0;    // first global colword of the batch
+};
+
+constexpr int kPhaseThreads = 128;
+
+// ---- encode, t >= 32 -------------------------------------------------------
+// E1: bottom IFFT of chunk c (message shards (c-1)t .. ct-1, coset omega_ct),
+// group g: variant v = (c - 1) * (t/16) + g = blockIdx.y.  Scratch row =
+// message row.
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kPhaseThreads) k_enc_p1(EncodeArgs a, Batch bt) {
+  constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
+  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  if (w >= bt.ncw) return;
+  const ShiftMul km = make_shift_mul();
+  const int v = blockIdx.y, c = v / G + 1, g = v % G;
+  uint32_t x[16][8];
 #pragma unroll
-    for (int s = 0; s < 2; s++) zero_rows(acc[s]);
-  }
-  for (int wv = 0; wv < WAVES; wv++) {
-    {  // bottom IFFT: warp -> (chunk in wave, group)
-      const int ci = warp / G, g = warp % G;
-      const int c = 1 + wv * WC + ci;
-      if (c <= C) {
-        uint32_t x[16][8];
+  for (int i = 0; i < 16; i++) gload(a.msg, (size_t)(c - 1) * T + 16 * g + i, a.L, bt.cw0 + w, x[i], km);
+  dispatch<0, C * G - 1>(v, [&](auto vv) {
+    constexpr int V = decltype(vv)::value;
+    block_ifft<0, 4, V % G, omega_c((V / G + 1) * T), 16>(x);
+  });
 #pragma unroll
-        for (int i = 0; i < 16; i++) gload(a.msg, (size_t)(c - 1) * T + 16 * g + i, a.L, col, x[i]);
-        dispatch<0, C * G - 1>((c - 1) * G + g, [&](auto v) {
-          constexpr int V = decltype(v)::value;
-          constexpr int CC = V / G + 1, GG = V % G;
-          block_ifft<0, 4, GG, omega_c(CC * T), 16>(x);
-        });
+  for (int i = 0; i < 16; i++) xstore(bt.s1, bt.ncw, (c - 1) * T + 16 * g + i, w, x[i]);
+}
+
+// E2: top levels for rows {b + 16 m} (b = blockIdx.y): IFFT top of every
+// chunk, accumulated, plus parity_in, then FFT top at 0; written to scratch
+// rows b + 16 m (chunk 1's rows, read above by this thread only).
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt) {
+  constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, TL = LOGT - 4, TR = 1 << TL;
+  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  if (w >= bt.ncw) return;
+  const int b = blockIdx.y;
+  uint32_t acc[TR][8];
+  zero_rows(acc);
+  for (int c = 1; c <= C; c++) {
+    uint32_t y[TR][8];
 #pragma unroll
-        for (int i = 0; i < 16; i++) sstore<32>(sm, ci * T + 16 * g + i, lane, x[i]);
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int s = 0; s < 2; s++) {  // top IFFT for b = warp + 8 s
-      const int b = warp + 8 * s;
-      uint32_t part[TR][8];
-      zero_rows(part);
-      for (int ci = 0; ci < WC; ci++) {
-        const int c = 1 + wv * WC + ci;
-        if (c > C) break;
-        uint32_t y[TR][8];
-#pragma unroll
-        for (int m = 0; m < TR; m++) sload<32>(sm, ci * T + b + 16 * m, lane, y[m]);
-        dispatch<1, C>(c, [&](auto cc) {
-          constexpr int CC = decltype(cc)::value;
-          block_ifft<4, TL, 0, omega_c(CC * T), TR>(y);
-        });
-#pragma unroll
-        for (int m = 0; m < TR; m++)
-#pragma unroll
-          for (int p = 0; p < 8; p++) part[m][p] ^= y[m][p];
-      }
-      if constexpr (WAVES > 1) {
-#pragma unroll
-        for (int m = 0; m < TR; m++)
-#pragma unroll
-          for (int p = 0; p < 8; p++) acc[s][m][p] ^= part[m][p];
-      } else {
-        // single wave: finish this b now (parity_in, top FFT, back to smem)
-        if (a.accumulate) {
-#pragma unroll
-          for (int m = 0; m < TR; m++) {
-            uint32_t q[8];
-            gload(a.parity, b + 16 * m, a.L, col, q);
-#pragma unroll
-            for (int p = 0; p < 8; p++) part[m][p] ^= q[p];
-          }
-        }
-        __syncwarp();
-        block_fft<4, TL, 0, 0, TR>(part);
-        // rows b + 16m of chunk 0's region were read above by this thread only
-#pragma unroll
-        for (int m = 0; m < TR; m++) sstore<32>(sm, b + 16 * m, lane, part[m]);
-      }
-    }
-    __syncthreads();
-  }
-  if constexpr (WAVES > 1) {
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      const int b = warp + 8 * s;
-      if (a.accumulate) {
-#pragma unroll
-        for (int m = 0; m < TR; m++) {
-          uint32_t q[8];
-          gload(a.parity, b + 16 * m, a.L, col, q);
-#pragma unroll
-          for (int p = 0; p < 8; p++) acc[s][m][p] ^= q[p];
-        }
-      }
-      block_fft<4, TL, 0, 0, TR>(acc[s]);
-#pragma unroll
-      for (int m = 0; m < TR; m++) sstore<32>(sm, b + 16 * m, lane, acc[s][m]);
-    }
-    __syncthreads();
-  }
-  if (warp < G) {  // bottom FFT and store
-    const int g = warp;
-    uint32_t x[16][8];
-#pragma unroll
-    for (int i = 0; i < 16; i++) sload<32>(sm, 16 * g + i, lane, x[i]);
-    dispatch<0, G - 1>(g, [&](auto v) {
-      constexpr int GG = decltype(v)::value;
-      block_fft<0, 4, GG, 0, 16>(x);
+    for (int m = 0; m < TR; m++) xload(bt.s1, bt.ncw, (c - 1) * T + b + 16 * m, w, y[m]);
+    dispatch<1, C>(c, [&](auto cc) {
+      constexpr int CC = decltype(cc)::value;
+      block_ifft<4, TL, 0, omega_c(CC * T), TR>(y);
     });
 #pragma unroll
-    for (int i = 0; i < 16; i++) gstore(a.parity, 16 * g + i, a.L, col, x[i]);
+    for (int m = 0; m < TR; m++)
+#pragma unroll
+      for (int p = 0; p < 8; p++) acc[m][p] ^= y[m][p];
   }
+  if (a.accumulate) {
+    const ShiftMul km = make_shift_mul();
+#pragma unroll
+    for (int m = 0; m < TR; m++) {
+      uint32_t q[8];
+      gload(a.parity, b + 16 * m, a.L, bt.cw0 + w, q, km);
+#pragma unroll
+      for (int p = 0; p < 8; p++) acc[m][p] ^= q[p];
+    }
+  }
+  block_fft<4, TL, 0, 0, TR>(acc);
+#pragma unroll
+  for (int m = 0; m < TR; m++) xstore(bt.s1, bt.ncw, b + 16 * m, w, acc[m]);
+}
+
+// E3: bottom FFT of group g = blockIdx.y and store of parity rows 16g..16g+15.
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kPhaseThreads) k_enc_p3(EncodeArgs a, Batch bt) {
+  constexpr int T = 1 << LOGT, G = T / 16;
+  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  if (w >= bt.ncw) return;
+  const ShiftMul km = make_shift_mul();
+  const int g = blockIdx.y;
+  uint32_t x[16][8];
+#pragma unroll
+  for (int i = 0; i < 16; i++) xload(bt.s1, bt.ncw, 16 * g + i, w, x[i]);
+  dispatch<0, G - 1>(g, [&](auto v) {
+    constexpr int GG = decltype(v)::value;
+    block_fft<0, 4, GG, 0, 16>(x);
+  });
+#pragma unroll
+  for (int i = 0; i < 16; i++) gstore(a.parity, 16 * g + i, a.L, bt.cw0 + w, x[i], km);
 }
 
 // ---- recover ------------------------------------------------------------
@@ -345,7 +366,8 @@ __global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t slice = (size_t)blockIdx.x * (kThreads / 32) + warp;
   if (slice * 1024 >= a.L) return;
-  const size_t col = (slice * 32 + lane) * 32;
+  const size_t cw = slice * 32 + lane;
+  const ShiftMul km = make_shift_mul();
   uint32_t x[N][8];
 #pragma unroll
   for (int r = 0; r < N; r++) {
@@ -353,8 +375,8 @@ __global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
 #pragma unroll
       for (int p = 0; p < 8; p++) x[r][p] = 0;
     } else {
-      gload(a.rx, r, a.L, col, x[r]);
-      scale_rt(x[r], s_lam[r]);
+      gload(a.rx, r, a.L, cw, x[r], km);
+      scale_rt(x[r], c_tab.exp[s_lam[r]]);
     }
   }
   block_ifft<0, LOGN, 0, 0, N>(x);
@@ -363,120 +385,148 @@ __global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
 #pragma unroll
   for (int r = 0; r < N; r++) {
     if (s_er[r]) {
-      scale_rt(x[r], s_ilp[r]);
-      gstore(a.rx, r, a.L, col, x[r]);
+      scale_rt(x[r], c_tab.exp[s_ilp[r]]);
+      gstore(a.rx, r, a.L, cw, x[r], km);
     }
   }
 }
 
-// n >= 32: one CTA per slice of CW colwords, all n rows bit-sliced in shared
-// memory.  The derivative splits over the row bits: D = D_top + D_bot, with
-// D_top acting on bits >= 4 (local to a top task) and D_bot on bits < 4
-// (read from the other tasks' rows in shared memory).  Top tasks run in
-// rounds of 16 colwords so that no task overwrites rows another task of the
-// same round still has to read.
-template <int LOGN, int CW>
-__global__ void __launch_bounds__(kThreads, 1) k_rec_large(RecoverArgs a) {
-  constexpr int N = 1 << LOGN, G = N / 16, TL = LOGN - 4, TR = 1 << TL;
-  extern __shared__ uint32_t sm[];  // N rows x 8 planes x CW colwords
+
+// n >= 32: three phase kernels.  With c' = IFFT_bot(y) and c = IFFT_top(c'),
+// the derivative splits over the row bits, D = D_top + D_bot, and D_bot
+// commutes with the top butterflies (its row pairs differ below every top
+// level, where no top twiddle depends), while FFT_top(c) = c'.  So
+//   FFT_n(D c) = FFT_bot(u + D_bot c'),  u = FFT_top(D_top c),
+// and with u' = FFT_top((I + D_top) c) = u + c' this is exactly
+//   FFT_n(D c) = FFT_bot(u' + (I + D_bot) c'),
+// where both I + D terms are computed in place (one_plus_derivative).
+//   R1: y = lambda .* r on group g, c' = IFFT_bot  -> s1
+//   R2: rows {b + 16m}: u' = FFT_top((I + D_top) IFFT_top(c'))  -> s2
+//   R3: group g with erasures: FFT_bot(s2 + (I + D_bot) s1), Forney, store.
+// Per-thread staging for rows that get a runtime scale: the scale runs in a
+// rolled loop (one copy of its code), the stage hands the rows to the
+// unrolled transform.  16 rows x 8 planes x kPhaseThreads words.
+__device__ __forceinline__ uint32_t* stage_at(uint32_t* st, int i, int p) {
+  return st + (i * 8 + p) * kPhaseThreads + threadIdx.x;
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(kPhaseThreads) k_rec_p1(RecoverArgs a, Batch bt) {
   __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
+  extern __shared__ uint32_t stage[];
   if (threadIdx.x < 32) erasure_locator_warp(a, c_tab, s_er, s_lam, s_ilp);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t col0 = (size_t)blockIdx.x * CW * 32;
-
-  // bottom IFFT: warp-uniform group g, lane = colword
-  for (int g = warp; g < G; g += kThreads / 32) {
-    if (lane < CW) {
-      const size_t col = col0 + (size_t)lane * 32;
-      uint32_t x[16][8];
-#pragma unroll
-      for (int i = 0; i < 16; i++) {
-        const int r = 16 * g + i;
-        if (s_er[r]) {
-#pragma unroll
-          for (int p = 0; p < 8; p++) x[i][p] = 0;
-        } else {
-          gload(a.rx, r, a.L, col, x[i]);
-          scale_rt(x[i], s_lam[r]);
-        }
-      }
-      dispatch<0, G - 1>(g, [&](auto v) {
-        constexpr int GG = decltype(v)::value;
-        block_ifft<0, 4, GG, 0, 16>(x);
-      });
-#pragma unroll
-      for (int i = 0; i < 16; i++) sstore<CW>(sm, 16 * g + i, lane, x[i]);
+  constexpr int G = (1 << LOGN) / 16;
+  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  if (w >= bt.ncw) return;
+  const ShiftMul km = make_shift_mul();
+  const int g = blockIdx.y;
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) {
+    const int r = 16 * g + i;
+    uint32_t y[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (!s_er[r]) {
+      gload(a.rx, r, a.L, bt.cw0 + w, y, km);
+      scale_log(y, s_lam[r]);
     }
+#pragma unroll
+    for (int p = 0; p < 8; p++) *stage_at(stage, i, p) = y[p];
   }
-  __syncthreads();
+  uint32_t x[16][8];
+#pragma unroll
+  for (int i = 0; i < 16; i++)
+#pragma unroll
+    for (int p = 0; p < 8; p++) x[i][p] = *stage_at(stage, i, p);
+  dispatch<0, G - 1>(g, [&](auto v) {
+    constexpr int GG = decltype(v)::value;
+    block_ifft<0, 4, GG, 0, 16>(x);
+  });
+#pragma unroll
+  for (int i = 0; i < 16; i++) xstore(bt.s1, bt.ncw, 16 * g + i, w, x[i]);
+}
 
-  // top pass in rounds of 16 colwords: task (b, w) = (tid / 16, 16 * round + tid % 16)
-  for (int w0 = 0; w0 < CW; w0 += 16) {
-    const int b = threadIdx.x >> 4;
-    const int w = w0 + (threadIdx.x & 15);
-    const bool active = w < CW;
-    uint32_t y[TR][8];
-    if (active) {
+template <int LOGN>
+__global__ void __launch_bounds__(kPhaseThreads) k_rec_p2(RecoverArgs a, Batch bt) {
+  constexpr int TL = LOGN - 4, TR = 1 << TL;
+  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  if (w >= bt.ncw) return;
+  const int b = blockIdx.y;
+  uint32_t y[TR][8];
 #pragma unroll
-      for (int m = 0; m < TR; m++) sload<CW>(sm, b + 16 * m, w, y[m]);
-      block_ifft<4, TL, 0, 0, TR>(y);
+  for (int m = 0; m < TR; m++) xload(bt.s1, bt.ncw, b + 16 * m, w, y[m]);
+  block_ifft<4, TL, 0, 0, TR>(y);
+  one_plus_derivative<TR>(y);
+  block_fft<4, TL, 0, 0, TR>(y);
 #pragma unroll
-      for (int m = 0; m < TR; m++) sstore<CW>(sm, b + 16 * m, w, y[m]);  // c, own rows
-    }
-    __syncthreads();
-    if (active) {
-      one_plus_derivative<TR>(y);  // (I + D_top) on the top index m
+  for (int m = 0; m < TR; m++) xstore(bt.s2, bt.ncw, b + 16 * m, w, y[m]);
+}
+
+// blockIdx.y indexes the list of groups holding at least one erasure.
+struct GroupList {
+  int count;
+  uint8_t g[16];
+};
+
+template <int LOGN>
+__global__ void __launch_bounds__(kPhaseThreads) k_rec_p3(RecoverArgs a, Batch bt, GroupList gl) {
+  __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
+  extern __shared__ uint32_t stage[];
+  if (threadIdx.x < 32) erasure_locator_warp(a, c_tab, s_er, s_lam, s_ilp);
+  __syncthreads();
+  constexpr int G = (1 << LOGN) / 16;
+  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  if (w >= bt.ncw) return;
+  const ShiftMul km = make_shift_mul();
+  const int g = gl.g[blockIdx.y];
+  uint32_t x[16][8];
 #pragma unroll
-      for (int j = 0; j < 4; j++) {  // + D_bot: rows b + 2^j for clear bits j of b
-        if ((b >> j) & 1) continue;
+  for (int i = 0; i < 16; i++) xload(bt.s1, bt.ncw, 16 * g + i, w, x[i]);
+  one_plus_derivative<16>(x);
 #pragma unroll
-        for (int m = 0; m < TR; m++) {
-          uint32_t q[8];
-          sload<CW>(sm, b + (1 << j) + 16 * m, w, q);
+  for (int i = 0; i < 16; i++) {
+    uint32_t q[8];
+    xload(bt.s2, bt.ncw, 16 * g + i, w, q);
 #pragma unroll
-          for (int p = 0; p < 8; p++) y[m][p] ^= q[p];
-        }
-      }
-    }
-    __syncthreads();
-    if (active) {
-      block_fft<4, TL, 0, 0, TR>(y);
-#pragma unroll
-      for (int m = 0; m < TR; m++) sstore<CW>(sm, b + 16 * m, w, y[m]);
-    }
+    for (int p = 0; p < 8; p++) x[i][p] ^= q[p];
   }
-  __syncthreads();
-
-  // bottom FFT, Forney scale, store the erased rows
-  for (int g = warp; g < G; g += kThreads / 32) {
-    bool any = false;
+  dispatch<0, G - 1>(g, [&](auto v) {
+    constexpr int GG = decltype(v)::value;
+    block_fft<0, 4, GG, 0, 16>(x);
+  });
 #pragma unroll
-    for (int i = 0; i < 16; i++) any |= s_er[16 * g + i] != 0;
-    if (!any || lane >= CW) continue;
-    const size_t col = col0 + (size_t)lane * 32;
-    uint32_t x[16][8];
+  for (int i = 0; i < 16; i++)
 #pragma unroll
-    for (int i = 0; i < 16; i++) sload<CW>(sm, 16 * g + i, lane, x[i]);
-    dispatch<0, G - 1>(g, [&](auto v) {
-      constexpr int GG = decltype(v)::value;
-      block_fft<0, 4, GG, 0, 16>(x);
-    });
+    for (int p = 0; p < 8; p++) *stage_at(stage, i, p) = x[i][p];
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) {
+    const int r = 16 * g + i;
+    if (!s_er[r]) continue;
+    uint32_t y[8];
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-      const int r = 16 * g + i;
-      if (s_er[r]) {
-        scale_rt(x[i], s_ilp[r]);
-        gstore(a.rx, r, a.L, col, x[i]);
-      }
-    }
+    for (int p = 0; p < 8; p++) y[p] = *stage_at(stage, i, p);
+    scale_log(y, s_ilp[r]);
+    gstore(a.rx, r, a.L, bt.cw0 + w, y, km);
   }
 }
 
 // ---- launchers ------------------------------------------------------------
 
+// Scratch budget per phase batch: both buffers together stay well inside L2.
+constexpr size_t kScratchBudget = (size_t)48 << 20;
+
+// Colwords covering L bytes in the io.cuh layout (whole 1024-column slices).
+inline size_t total_colwords(size_t L) { return (L + 1023) / 1024 * 32; }
+
+inline size_t batch_colwords(size_t rows_per_buffer, int buffers, size_t scratch_bytes, size_t total_cw) {
+  const size_t per_cw = rows_per_buffer * 32 * (size_t)buffers;
+  size_t cap = scratch_bytes < kScratchBudget ? scratch_bytes : kScratchBudget;
+  size_t cw = cap / per_cw;
+  if (cw > total_cw) cw = total_cw;
+  return cw;
+}
+
 template <int LOGN, int LOGT>
-cudaError_t launch_enc(const EncodeArgs& a, cudaStream_t s) {
+cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
   if constexpr (LOGT <= 4) {
     constexpr size_t smem = (LOGT == 4) ? (size_t)8 * 16 * 8 * 32 * 4 : 0;
     auto fn = k_enc_small<LOGN, LOGT>;
@@ -486,36 +536,68 @@ cudaError_t launch_enc(const EncodeArgs& a, cudaStream_t s) {
     }
     const size_t slices = (a.L + 1023) / 1024;
     fn<<<(unsigned)((slices + 7) / 8), kThreads, smem, s>>>(a);
+    return cudaGetLastError();
   } else {
-    constexpr size_t smem = (size_t)128 * 8 * 32 * 4;
-    auto fn = k_enc_large<LOGN, LOGT>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    fn<<<(unsigned)((a.L + 1023) / 1024), kThreads, smem, s>>>(a);
+    constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
+    const size_t total_cw = total_colwords(a.L);
+    const size_t bcw = batch_colwords(N - T, 1, sc.bytes, total_cw);
+    if (bcw == 0) return cudaErrorMemoryAllocation;
+    for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
+      Batch bt{sc.ptr, nullptr, (total_cw - cw0 < bcw ? total_cw - cw0 : bcw), cw0};
+      const unsigned gx = (unsigned)((bt.ncw + kPhaseThreads - 1) / kPhaseThreads);
+      k_enc_p1<LOGN, LOGT><<<dim3(gx, C * G), kPhaseThreads, 0, s>>>(a, bt);
+      k_enc_p2<LOGN, LOGT><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
+      k_enc_p3<LOGN, LOGT><<<dim3(gx, G), kPhaseThreads, 0, s>>>(a, bt);
+    }
+    return cudaGetLastError();
   }
-  return cudaGetLastError();
 }
 
 template <int LOGN>
-cudaError_t launch_rec(const RecoverArgs& a, cudaStream_t s) {
+cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s) {
   if constexpr (LOGN <= 4) {
     const size_t slices = (a.L + 1023) / 1024;
     k_rec_small<LOGN><<<(unsigned)((slices + 7) / 8), kThreads, 0, s>>>(a);
+    return cudaGetLastError();
   } else {
-    constexpr int CW = LOGN == 8 ? 24 : 32;
-    constexpr size_t smem = (size_t)(1 << LOGN) * 8 * CW * 4;
-    auto fn = k_rec_large<LOGN, CW>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    constexpr int N = 1 << LOGN, G = N / 16;
+    GroupList gl{};
+    bool has[16] = {};
+    for (int j = 0; j < a.e; j++) has[a.pos[j] >> 4] = true;
+    for (int g = 0; g < G; g++)
+      if (has[g]) gl.g[gl.count++] = (uint8_t)g;
+    const size_t total_cw = total_colwords(a.L);
+    const size_t bcw = batch_colwords(N, 2, sc.bytes, total_cw);
+    if (bcw == 0) return cudaErrorMemoryAllocation;
+    constexpr size_t stage_bytes = (size_t)16 * 8 * kPhaseThreads * 4;
+    cudaError_t e = cudaFuncSetAttribute(k_rec_p1<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_rec_p3<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
     if (e != cudaSuccess) return e;
-    fn<<<(unsigned)((a.L + CW * 32 - 1) / (CW * 32)), kThreads, smem, s>>>(a);
+    for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
+      const size_t ncw = total_cw - cw0 < bcw ? total_cw - cw0 : bcw;
+      Batch bt{sc.ptr, sc.ptr + (size_t)N * ncw * 8, ncw, cw0};
+      const unsigned gx = (unsigned)((ncw + kPhaseThreads - 1) / kPhaseThreads);
+      k_rec_p1<LOGN><<<dim3(gx, G), kPhaseThreads, stage_bytes, s>>>(a, bt);
+      k_rec_p2<LOGN><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
+      k_rec_p3<LOGN><<<dim3(gx, gl.count), kPhaseThreads, stage_bytes, s>>>(a, bt, gl);
+    }
+    return cudaGetLastError();
   }
-  return cudaGetLastError();
 }
+
+// Scratch bytes a call needs for one batch covering the whole shard
+// (callers may provide less: the launchers then batch the columns).
+inline size_t scratch_full_bytes_enc(int n, int t, size_t L) {
+  return t >= 32 ? (size_t)(n - t) * total_colwords(L) * 32 : 0;
+}
+inline size_t scratch_full_bytes_rec(int n, size_t L) { return n >= 32 ? (size_t)2 * n * total_colwords(L) * 32 : 0; }
 
 // Per-shape entry points, one translation unit each (special_enc_*.cu,
 // special_rec_*.cu) so that the build parallelises.
-#define AFRS_DECLARE_ENC(LN, LT) cudaError_t launch_enc_##LN##_##LT(const EncodeArgs& a, cudaStream_t s);
-#define AFRS_DECLARE_REC(LN) cudaError_t launch_rec_##LN(const RecoverArgs& a, cudaStream_t s);
+#define AFRS_DECLARE_ENC(LN, LT) \
+  cudaError_t launch_enc_##LN##_##LT(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s);
+#define AFRS_DECLARE_REC(LN) cudaError_t launch_rec_##LN(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s);
 AFRS_DECLARE_ENC(1, 0)
 AFRS_DECLARE_ENC(2, 0)
 AFRS_DECLARE_ENC(2, 1)

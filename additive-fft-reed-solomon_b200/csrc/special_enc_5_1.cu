@@ -1,8 +1,10 @@
-// Encode kernel for n = 32, t = 2.
+// Encode kernels for n = 32, t = 2.
 #include "special.cuh"
 
 namespace afrs {
 namespace spec {
-cudaError_t launch_enc_5_1(const EncodeArgs& a, cudaStream_t s) { return launch_enc<5, 1>(a, s); }
+cudaError_t launch_enc_5_1(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
+  return launch_enc<5, 1>(a, sc, s);
+}
 }  // namespace spec
 }  // namespace afrs

@@ -1,8 +1,10 @@
-// Encode kernel for n = 128, t = 4.
+// Encode kernels for n = 128, t = 4.
 #include "special.cuh"
 
 namespace afrs {
 namespace spec {
-cudaError_t launch_enc_7_2(const EncodeArgs& a, cudaStream_t s) { return launch_enc<7, 2>(a, s); }
+cudaError_t launch_enc_7_2(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
+  return launch_enc<7, 2>(a, sc, s);
+}
 }  // namespace spec
 }  // namespace afrs

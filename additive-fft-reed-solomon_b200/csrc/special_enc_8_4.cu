@@ -1,8 +1,10 @@
-// Encode kernel for n = 256, t = 16.
+// Encode kernels for n = 256, t = 16.
 #include "special.cuh"
 
 namespace afrs {
 namespace spec {
-cudaError_t launch_enc_8_4(const EncodeArgs& a, cudaStream_t s) { return launch_enc<8, 4>(a, s); }
+cudaError_t launch_enc_8_4(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
+  return launch_enc<8, 4>(a, sc, s);
+}
 }  // namespace spec
 }  // namespace afrs

@@ -1,8 +1,10 @@
-// Recover kernel for n = 8.
+// Recover kernels for n = 8.
 #include "special.cuh"
 
 namespace afrs {
 namespace spec {
-cudaError_t launch_rec_3(const RecoverArgs& a, cudaStream_t s) { return launch_rec<3>(a, s); }
+cudaError_t launch_rec_3(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s) {
+  return launch_rec<3>(a, sc, s);
+}
 }  // namespace spec
 }  // namespace afrs

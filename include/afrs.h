@@ -65,7 +65,11 @@ int afrs_recover(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* received, size_
 
 /* Device-pointer variants of the two calls above, enqueued on `stream`
  * (a cudaStream_t; NULL = the legacy default stream).  Positions are read
- * from host memory during the call.  They allocate nothing. */
+ * from host memory during the call.  For t >= 32 (encode) and n >= 32
+ * (recover) the kernels keep intermediate rows in a device scratch buffer
+ * owned by the context: the first call of a size grows it (at most 48 MiB;
+ * longer shards are processed in column batches), and calls that share a
+ * context are ordered on that buffer even when they use different streams. */
 int afrs_encode_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, const uint8_t* d_message,
                     uint8_t* d_parity, size_t shard_len, int accumulate, void* stream);
 int afrs_recover_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* d_received,
