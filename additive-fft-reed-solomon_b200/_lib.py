@@ -33,6 +33,7 @@ SIGNATURES = {
     "afrs_fft_sharded_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _sz, _u32, ctypes.c_uint8, ctypes.c_void_p]),
     "afrs_ifft_sharded_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _sz, _u32, ctypes.c_uint8, ctypes.c_void_p]),
     "afrs_scale_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _u8p, _sz, ctypes.c_uint8, ctypes.c_void_p]),
+    "afrs_recover_dev_noalloc": (ctypes.c_int, [_u32, _u32, _u8p, _sz, _u8p, _sz, ctypes.c_void_p]),
 }
 
 

@@ -131,6 +131,10 @@ int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
 
 }  // namespace
 
+namespace afrs {
+void set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+}  // namespace afrs
+
 extern "C" {
 
 const char* afrs_last_error(void) { return g_err; }

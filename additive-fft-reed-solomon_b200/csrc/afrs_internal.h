@@ -46,6 +46,8 @@ struct ScratchArena {
 cudaError_t launch_encode_special(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s);
 cudaError_t launch_recover_special(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s);
 size_t scratch_bytes_encode(int n, int t, size_t L);
+// Sets the calling thread's afrs_last_error() message.
+void set_last_error(const char* msg);
 size_t scratch_bytes_recover(int n, size_t L);
 
 }  // namespace afrs

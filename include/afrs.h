@@ -91,6 +91,25 @@ int afrs_ifft_sharded_dev(afrs_ctx* ctx, uint8_t* d_shards, size_t shard_len, ui
 int afrs_scale_dev(afrs_ctx* ctx, const uint8_t* d_src, uint8_t* d_dst, size_t len, uint8_t scalar,
                    void* stream);
 
+/* Allocation-free erasure recovery.  No counterpart in the reference: it
+ * exists for callers that cannot allocate device memory when they recover,
+ * e.g. code inside CUDA stream capture (cudaMalloc is not allowed there),
+ * serving loops that must never wait on the device-wide synchronisation an
+ * allocation may take, and hosts that give the library a fixed memory
+ * budget.  Same arguments and results as afrs_recover_dev, on the current
+ * device, without a context.  Its scratch is a 32 MiB array of device
+ * memory compiled into the library (held by every GPU that loads it, until
+ * the process exits); shards that need more (n * ceil(shard_len/1024) * 2 KiB
+ * > 32 MiB for n >= 32, e.g. n = 256 with shard_len > 64 KiB) are refused
+ * with AFRS_EINVAL and a message in afrs_last_error().  The first call on a
+ * device looks up the array's device address (a set-up step), so make it
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (different streams, or different host threads) race and
+ * must be ordered by the caller.  No scratch word needs clearing between
+ * calls: each call writes every word it reads. */
+int afrs_recover_dev_noalloc(uint32_t n, uint32_t t, uint8_t* d_received, size_t shard_len,
+                             const uint8_t* positions, size_t e, void* stream);
+
 /* Library build information (kernel set, arch) for logs. */
 const char* afrs_version(void);
 
