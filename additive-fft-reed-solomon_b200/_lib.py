@@ -19,6 +19,18 @@ _u8p = ctypes.c_void_p
 _sz = ctypes.c_size_t
 _u32 = ctypes.c_uint32
 
+AFRS_OP_ENCODE = 0
+AFRS_OP_RECOVER = 1
+
+
+class AfrsJob(ctypes.Structure):
+    """struct afrs_job of include/afrs.h."""
+
+    _fields_ = [("op", ctypes.c_uint32), ("n", ctypes.c_uint32), ("t", ctypes.c_uint32), ("e", ctypes.c_uint32),
+                ("shard_len", ctypes.c_size_t), ("src", ctypes.c_void_p), ("dst", ctypes.c_void_p),
+                ("positions", ctypes.c_uint8 * 256), ("status", ctypes.c_int32), ("reserved", ctypes.c_uint32)]
+
+
 # name -> (restype, argtypes); the list mirrors include/afrs.h.
 SIGNATURES = {
     "afrs_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
@@ -34,6 +46,7 @@ SIGNATURES = {
     "afrs_ifft_sharded_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _sz, _u32, ctypes.c_uint8, ctypes.c_void_p]),
     "afrs_scale_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _u8p, _sz, ctypes.c_uint8, ctypes.c_void_p]),
     "afrs_recover_dev_noalloc": (ctypes.c_int, [_u32, _u32, _u8p, _sz, _u8p, _sz, ctypes.c_void_p]),
+    "afrs_batch_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AfrsJob), _sz, ctypes.c_void_p]),
 }
 
 

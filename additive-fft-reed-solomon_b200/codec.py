@@ -26,7 +26,7 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["AfrsError", "Context", "Codec", "fft_sharded", "ifft_sharded", "scale"]
+__all__ = ["AfrsError", "Context", "Codec", "Job", "run_batch", "fft_sharded", "ifft_sharded", "scale"]
 
 
 class AfrsError(RuntimeError):
@@ -186,3 +186,50 @@ def scale(src, dst, scalar: int, device: int = 0) -> None:
     ctx = Context.get(device)
     _check(_lib.lib().afrs_scale_dev(ctx.handle, _dev_ptr(src), _dev_ptr(dst), src.numel(), scalar, _stream(src)),
            "scale")
+
+
+class Job:
+    """One codeword of a batch: ``Job.encode(n, t, message, parity, shard_len)``
+    or ``Job.recover(n, t, received, shard_len, positions)`` on uint8 CUDA
+    tensors.  After ``run_batch`` its ``status`` is the C ABI's job status."""
+
+    def __init__(self, op, n, t, src, dst, shard_len, positions=()):
+        self.op, self.n, self.t, self.src, self.dst, self.shard_len = op, int(n), int(t), src, dst, int(shard_len)
+        self.positions = [int(p) for p in positions]
+        self.status = None
+
+    @classmethod
+    def encode(cls, n, t, message, parity, shard_len):
+        return cls(_lib.AFRS_OP_ENCODE, n, t, message, parity, shard_len)
+
+    @classmethod
+    def recover(cls, n, t, received, shard_len, positions):
+        return cls(_lib.AFRS_OP_RECOVER, n, t, None, received, shard_len, positions)
+
+    @property
+    def nbytes(self) -> int:
+        return self.n * self.shard_len
+
+
+def run_batch(jobs, device: int = 0, stream=None) -> list:
+    """Enqueue every job in one batched launch (afrs_batch_dev) on the
+    current torch stream (or ``stream``); returns the per-job statuses."""
+    import torch
+
+    arr = (_lib.AfrsJob * max(len(jobs), 1))()
+    for i, j in enumerate(jobs):
+        a = arr[i]
+        a.op, a.n, a.t, a.shard_len = j.op, j.n, j.t, j.shard_len
+        a.e = len(j.positions)
+        for q, p in enumerate(j.positions[:256]):
+            a.positions[q] = p
+        a.src = _dev_ptr(j.src) if j.src is not None else None
+        a.dst = _dev_ptr(j.dst) if j.dst is not None else None
+    ctx = Context.get(device)
+    s = stream if stream is not None else torch.cuda.current_stream(device)
+    _check(_lib.lib().afrs_batch_dev(ctx.handle, arr, len(jobs), s.cuda_stream), "afrs_batch_dev")
+    out = []
+    for i, j in enumerate(jobs):
+        j.status = int(arr[i].status)
+        out.append(j.status)
+    return out

@@ -4,7 +4,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "../../include/afrs.h"
 #include "afrs_internal.h"
@@ -17,6 +19,14 @@ struct afrs_ctx {
   uint32_t* work;  // bit-sliced intermediate rows of the phase kernels
   size_t work_bytes;
   cudaEvent_t work_free;  // recorded after each use of `work`
+  // Descriptor tables of afrs_batch_dev, two slots so that one batch can be
+  // prepared while the previous one runs.
+  uint8_t* batch_dev[2];
+  size_t batch_dev_bytes[2];
+  uint8_t* batch_host[2];  // pinned staging of those tables
+  size_t batch_host_bytes[2];
+  cudaEvent_t batch_free[2];  // recorded after each batch of the slot
+  int batch_slot;
   std::recursive_mutex mu;
 };
 
@@ -156,12 +166,21 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
   c->scratch_bytes = 0;
   c->work = nullptr;
   c->work_bytes = 0;
+  for (int i = 0; i < 2; i++) {
+    c->batch_dev[i] = nullptr;
+    c->batch_dev_bytes[i] = 0;
+    c->batch_host[i] = nullptr;
+    c->batch_host_bytes[i] = 0;
+  }
+  c->batch_slot = 0;
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;
     return cuda_fail(e, "cudaStreamCreate");
   }
   e = cudaEventCreateWithFlags(&c->work_free, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->batch_free[0], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->batch_free[1], cudaEventDisableTiming);
   if (e != cudaSuccess) {
     cudaStreamDestroy(c->stream);
     delete c;
@@ -177,6 +196,11 @@ void afrs_ctx_destroy(afrs_ctx* c) {
   cudaDeviceSynchronize();
   if (c->scratch) cudaFree(c->scratch);
   if (c->work) cudaFree(c->work);
+  for (int i = 0; i < 2; i++) {
+    if (c->batch_dev[i]) cudaFree(c->batch_dev[i]);
+    if (c->batch_host[i]) cudaFreeHost(c->batch_host[i]);
+    cudaEventDestroy(c->batch_free[i]);
+  }
   cudaEventDestroy(c->work_free);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -317,6 +341,123 @@ int afrs_scale_dev(afrs_ctx* c, const uint8_t* src, uint8_t* dst, size_t len, ui
   DeviceGuard g(c->device);
   cudaError_t e = afrs::launch_scale(src, dst, len, scalar, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "scale launch");
+}
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (count && !jobs) return fail(AFRS_EINVAL, "jobs is NULL");
+  if (count > (size_t)1 << 24) return fail(AFRS_EINVAL, "too many jobs (%zu)", count);
+  std::vector<afrs::BatchJob> bj;
+  std::vector<uint2> tasks;
+  std::vector<int> rec;
+  std::vector<uint8_t> pos;
+  int max_rows = 0;
+  for (size_t i = 0; i < count; i++) {
+    afrs_job& j = jobs[i];
+    j.status = AFRS_EINVAL;
+    if (j.op != AFRS_OP_ENCODE && j.op != AFRS_OP_RECOVER) continue;
+    if (!pow2(j.n) || j.n < 2 || j.n > 256 || !pow2(j.t) || j.t >= j.n) continue;
+    const bool enc = j.op == AFRS_OP_ENCODE;
+    if (!enc) {
+      if (j.e > j.t) {
+        j.status = 0;
+        continue;
+      }
+      bool seen[256] = {}, ok = true;
+      for (uint32_t q = 0; q < j.e; q++) {
+        if (j.positions[q] >= j.n || seen[j.positions[q]]) ok = false;
+        else seen[j.positions[q]] = true;
+      }
+      if (!ok) continue;
+      if (j.e == 0 || j.shard_len == 0) {
+        j.status = 1;
+        continue;
+      }
+      if (!j.dst) continue;
+    } else {
+      if (j.shard_len == 0) {
+        j.status = 0;
+        continue;
+      }
+      if (!j.src || !j.dst) continue;
+    }
+    afrs::BatchJob b{};
+    b.src = j.src;
+    b.dst = j.dst;
+    b.L = j.shard_len;
+    b.op = enc ? 0 : 1;
+    b.n = (int)j.n;
+    b.t = (int)j.t;
+    b.e = (int)j.e;
+    b.pos_off = (uint32_t)pos.size();
+    if (!enc) {
+      b.loc = (uint32_t)rec.size();
+      rec.push_back((int)bj.size());
+      pos.insert(pos.end(), j.positions, j.positions + j.e);
+      max_rows = std::max(max_rows, 2 * (int)j.n);
+    } else {
+      max_rows = std::max(max_rows, (int)j.t * ((int)(j.n / j.t) - 1 > 1 ? 2 : 1));
+    }
+    const size_t tiles = afrs::batch_tiles(j.shard_len);
+    for (size_t q = 0; q < tiles; q++) tasks.push_back(make_uint2((unsigned)bj.size(), (unsigned)q));
+    j.status = enc ? 0 : 1;
+    bj.push_back(b);
+  }
+  if (tasks.size() > (size_t)INT32_MAX) return fail(AFRS_EINVAL, "too many tiles");
+  if (bj.empty()) return AFRS_OK;
+  const size_t o_jobs = 0;
+  const size_t o_tasks = align256(o_jobs + bj.size() * sizeof(afrs::BatchJob));
+  const size_t o_rec = align256(o_tasks + tasks.size() * sizeof(uint2));
+  const size_t o_pos = align256(o_rec + rec.size() * sizeof(int));
+  const size_t o_cnt = align256(o_pos + pos.size() + 1);
+  const size_t upload = o_cnt;  // the locator table and the counter are written on the device
+  const size_t o_loc = align256(o_cnt + sizeof(unsigned));
+  const size_t total = align256(o_loc + rec.size() * 768);
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  DeviceGuard g(c->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int slot = c->batch_slot;
+  c->batch_slot ^= 1;
+  // The slot's previous batch must be done with its staging and tables.
+  cudaError_t e = cudaEventSynchronize(c->batch_free[slot]);
+  if (e != cudaSuccess) return cuda_fail(e, "batch wait");
+  if (total > c->batch_dev_bytes[slot]) {
+    if (c->batch_dev[slot]) cudaFree(c->batch_dev[slot]);
+    c->batch_dev[slot] = nullptr;
+    c->batch_dev_bytes[slot] = 0;
+    if ((e = cudaMalloc(&c->batch_dev[slot], total * 2)) != cudaSuccess) return cuda_fail(e, "batch tables");
+    c->batch_dev_bytes[slot] = total * 2;
+  }
+  if (upload > c->batch_host_bytes[slot]) {
+    if (c->batch_host[slot]) cudaFreeHost(c->batch_host[slot]);
+    c->batch_host[slot] = nullptr;
+    c->batch_host_bytes[slot] = 0;
+    if ((e = cudaMallocHost(&c->batch_host[slot], upload * 2)) != cudaSuccess) return cuda_fail(e, "batch staging");
+    c->batch_host_bytes[slot] = upload * 2;
+  }
+  uint8_t* h = c->batch_host[slot];
+  std::memcpy(h + o_jobs, bj.data(), bj.size() * sizeof(afrs::BatchJob));
+  std::memcpy(h + o_tasks, tasks.data(), tasks.size() * sizeof(uint2));
+  if (!rec.empty()) std::memcpy(h + o_rec, rec.data(), rec.size() * sizeof(int));
+  if (!pos.empty()) std::memcpy(h + o_pos, pos.data(), pos.size());
+  uint8_t* d = c->batch_dev[slot];
+  if ((e = cudaMemcpyAsync(d, h, upload, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_fail(e, "batch upload");
+  afrs::BatchLaunch bl{};
+  bl.jobs = reinterpret_cast<const afrs::BatchJob*>(d + o_jobs);
+  bl.tasks = reinterpret_cast<const uint2*>(d + o_tasks);
+  bl.ntasks = (int)tasks.size();
+  bl.rec_jobs = reinterpret_cast<const int*>(d + o_rec);
+  bl.nrec = (int)rec.size();
+  bl.pos_tab = d + o_pos;
+  bl.loc_tab = d + o_loc;
+  bl.counter = reinterpret_cast<unsigned*>(d + o_cnt);
+  bl.max_rows = max_rows;
+  if ((e = afrs::launch_batch(bl, s)) != cudaSuccess) return cuda_fail(e, "batch launch");
+  if ((e = cudaEventRecord(c->batch_free[slot], s)) != cudaSuccess) return cuda_fail(e, "batch record");
+  return AFRS_OK;
 }
 
 }  // extern "C"

@@ -24,6 +24,31 @@ struct EncodeArgs {
   int accumulate;
 };
 
+// Batched launch (batch.cu): device tables built by afrs_batch_dev.
+struct BatchJob {
+  const uint8_t* src;  // encode: message; recover: the codeword
+  uint8_t* dst;        // encode: parity; recover: the codeword (same as src)
+  size_t L;
+  int op, n, t, e;     // op 0 = encode, 1 = recover
+  uint32_t pos_off;    // erasure positions at pos_tab + pos_off
+  uint32_t loc;        // locator slot of a recover job
+};
+
+struct BatchLaunch {
+  const BatchJob* jobs;
+  const uint2* tasks;    // (job, 256-column tile)
+  int ntasks;
+  const int* rec_jobs;   // indices of the recover jobs
+  int nrec;
+  const uint8_t* pos_tab;
+  uint8_t* loc_tab;      // nrec * 768 bytes
+  unsigned* counter;     // task counter (reset by the launch)
+  int max_rows;          // largest 2n (recover) or 2t (encode) over the jobs
+};
+
+size_t batch_tiles(size_t L);
+cudaError_t launch_batch(const BatchLaunch& b, cudaStream_t s);
+
 // Generic kernels: any (n, t), runtime twiddles.
 cudaError_t launch_encode_generic(const EncodeArgs& a, cudaStream_t s);
 cudaError_t launch_recover_generic(const RecoverArgs& a, cudaStream_t s);

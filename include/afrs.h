@@ -91,6 +91,33 @@ int afrs_ifft_sharded_dev(afrs_ctx* ctx, uint8_t* d_shards, size_t shard_len, ui
 int afrs_scale_dev(afrs_ctx* ctx, const uint8_t* d_src, uint8_t* d_dst, size_t len, uint8_t scalar,
                    void* stream);
 
+/* Batched path: many independent codewords of any shapes in one persistent
+ * launch (no counterpart in the reference, whose methods take one codeword;
+ * each job is one call of encode_systematic_sharded, rs/src/codec.rs:241-265,
+ * or recover_erasure_shards, :479-569).  Device buffers.  Encode jobs write
+ * parity (parity_in is treated as zero, i.e. accumulate = 0); recover jobs
+ * rewrite the erased shards of dst (src is ignored; erased shards need not be
+ * zero).  Each job's status is set during the call: encode 0 = queued; recover
+ * 1 = queued, 0 = more erasures than t (nothing written, the reference's
+ * false); < 0 = rejected (AFRS_EINVAL), nothing written.  The call returns
+ * AFRS_OK once the batch is enqueued on `stream`, or < 0 when nothing was.
+ * The descriptor tables live in the context; successive batches on one
+ * context are ordered even across streams. */
+#define AFRS_OP_ENCODE 0u
+#define AFRS_OP_RECOVER 1u
+typedef struct afrs_job {
+  uint32_t op;      /* AFRS_OP_ENCODE or AFRS_OP_RECOVER */
+  uint32_t n, t;    /* shards, parity shards */
+  uint32_t e;       /* recover: number of erasures */
+  size_t shard_len; /* bytes per shard */
+  const uint8_t* src; /* encode: (n-t)*shard_len message bytes */
+  uint8_t* dst;       /* encode: t*shard_len parity bytes; recover: n*shard_len codeword */
+  uint8_t positions[256]; /* recover: erased shard indices (first e) */
+  int32_t status;         /* out */
+  uint32_t reserved;
+} afrs_job;
+int afrs_batch_dev(afrs_ctx* ctx, afrs_job* jobs, size_t count, void* stream);
+
 /* Allocation-free erasure recovery.  No counterpart in the reference: it
  * exists for callers that cannot allocate device memory when they recover,
  * e.g. code inside CUDA stream capture (cudaMalloc is not allowed there),

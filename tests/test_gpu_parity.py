@@ -201,3 +201,61 @@ def test_recompute_data_from_parity(afrs, t):
     d = torch.from_numpy(rx).cuda()
     afrs.Codec(n, t).recompute_data_from_parity_sharded(d, None, L)
     assert (d.cpu().numpy() == cw).all()
+
+
+def _batch_mix(afrs, count, seed, max_len=4096):
+    """A config-3-like mix: n in {32..256}, t in {4, 8, n/4, n/2}, shard
+    lengths log-uniform (multiples of 64 B and ragged ones), e in 1..t."""
+    rng = np.random.default_rng(seed)
+    jobs, expect = [], []
+    for i in range(count):
+        n = int(rng.choice([2, 4, 16, 32, 64, 128, 256]))
+        t = int(rng.choice([c for c in (1, 2, 4, 8, n // 4, n // 2) if 1 <= c < n]))
+        L = int(np.exp(rng.uniform(np.log(1), np.log(max_len))))
+        msg = oracle.random_bytes((n - t) * L, seed * 10007 + i)
+        par = np.zeros(t * L, np.uint8)
+        oracle.encode_systematic_sharded(n, t, msg, par, L)
+        if i % 2 == 0:
+            d_par = torch.full((t * L,), 0xA5, dtype=torch.uint8, device="cuda")
+            jobs.append(afrs.Job.encode(n, t, torch.from_numpy(msg).cuda(), d_par, L))
+            expect.append(par)
+        else:
+            cw = np.concatenate([par, msg])
+            e = int(rng.integers(1, t + 1))
+            pos = rng.choice(n, e, replace=False).tolist()
+            rx = cw.copy()
+            for p in pos:
+                rx[p * L:(p + 1) * L] = 0x5A  # erased rows need not be zero here
+            jobs.append(afrs.Job.recover(n, t, torch.from_numpy(rx).cuda(), L, pos))
+            expect.append(cw)
+    return jobs, expect
+
+
+@pytest.mark.gpu
+def test_batch_matches_oracle_on_mixed_shapes(afrs):
+    jobs, expect = _batch_mix(afrs, 120, seed=3)
+    status = afrs.run_batch(jobs)
+    torch.cuda.synchronize()
+    for j, ex, st in zip(jobs, expect, status):
+        assert st == (0 if j.op == 0 else 1)
+        assert (j.dst.cpu().numpy() == ex).all(), (j.op, j.n, j.t, j.shard_len)
+
+
+@pytest.mark.gpu
+def test_batch_equals_per_call_path_and_reports_status(afrs):
+    jobs, expect = _batch_mix(afrs, 40, seed=9, max_len=700)
+    bad = afrs.Job.recover(64, 8, torch.zeros(64 * 10, dtype=torch.uint8, device="cuda"), 10, [3, 3])
+    too_many = afrs.Job.recover(64, 8, torch.zeros(64 * 10, dtype=torch.uint8, device="cuda"), 10, list(range(9)))
+    status = afrs.run_batch(jobs + [bad, too_many])
+    torch.cuda.synchronize()
+    assert status[-2] == afrs._lib.AFRS_EINVAL and status[-1] == 0
+    for j, ex in zip(jobs, expect):
+        if j.op == 0:
+            ref = torch.zeros_like(j.dst)
+            afrs.Codec(j.n, j.t).encode_parity(j.src, ref, j.shard_len)
+        else:
+            ref = torch.from_numpy(ex.copy()).cuda()
+            for p in j.positions:
+                ref[p * j.shard_len:(p + 1) * j.shard_len] = 0
+            afrs.Codec(j.n, j.t).recover_erasure_shards(ref, None, j.shard_len, j.positions)
+        assert torch.equal(ref, j.dst)
