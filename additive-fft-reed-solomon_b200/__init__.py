@@ -11,3 +11,4 @@ from .codec import AfrsError, Codec, Context, Job, fft_sharded, ifft_sharded, ru
 # The reference's type names for the same codec (rs/src/lib.rs:20-45).
 Rs = Codec
 RsCuda = Codec
+from . import serving  # noqa: F401,E402

@@ -8,6 +8,7 @@ Inputs rotate over enough codewords that every step reads data that is not
 in L2.  Prints one JSON line (rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py --workload {small,batched,serving,large}   (other configs)
 
 --impl reference times the reference's CPU algorithm instead: the reference
 is a Rust crate and no Rust toolchain exists here, so its GFNI kernel
@@ -149,10 +150,15 @@ def main():
     ap.add_argument("--impl", default="afrs", choices=["afrs", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="codeword", choices=["codeword", "small", "batched", "serving", "large"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "codeword":
+        import bench_workloads  # noqa: E402  (secondary configurations)
+
+        return bench_workloads.run(args.workload, args)
 
     import numpy as np
     import torch

@@ -1,0 +1,261 @@
+"""Secondary benchmark workloads of bench.py (one JSON line each):
+
+  small    n=64, k=32, 1 KiB shards: encode + recover 32 random erasures
+  batched  4096 codewords of mixed shapes in one batched launch vs the
+           per-call path (n in {32,64,128,256}, t in {4,8,n/4,n/2},
+           shard length log-uniform 64 B..16 KiB in 64 B steps, e in 1..t,
+           half encode, half recover)
+  serving  open-loop Poisson stream of those requests plus a 5% tail of
+           n=256, k=192 codewords with 1 MiB shards, offered load swept
+           from 10% to 120% of the batched capacity, batched (continuous
+           batching) vs per-call serving, 32 GiB admission cap
+  large    n=256, k=224 (t=32), 4 MiB shards (1 GiB codeword): encode, then
+           recover 32 erasures (a) inside the message shards and (b) as one
+           contiguous run, with a bit-exact round-trip check on device
+
+Bytes are n*L per codeword operation.  Data are synthetic (seeded).
+"""
+from __future__ import annotations
+
+import json
+import math
+import time
+
+import numpy as np
+
+
+def _pkg():
+    import __graft_entry__
+
+    return __graft_entry__.load_package()
+
+
+def _events():
+    import torch
+
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _shape(rng):
+    n = int(rng.choice([32, 64, 128, 256]))
+    t = int(rng.choice([4, 8, n // 4, n // 2]))
+    L = int(round(math.exp(rng.uniform(math.log(64), math.log(16384))) / 64)) * 64
+    return n, t, max(L, 64)
+
+
+def _make_jobs(afrs, count, seed, tail_frac=0.0):
+    """Jobs on random device data (recover work does not depend on whether
+    the survivors form a codeword; correctness is covered by the tests)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    jobs = []
+    for i in range(count):
+        if tail_frac and rng.random() < tail_frac:
+            n, t, L = 256, 64, 1 << 20
+        else:
+            n, t, L = _shape(rng)
+        if i % 2 == 0:
+            src = torch.randint(0, 256, ((n - t) * L,), dtype=torch.uint8, device="cuda", generator=g)
+            dst = torch.empty(t * L, dtype=torch.uint8, device="cuda")
+            jobs.append(afrs.Job.encode(n, t, src, dst, L))
+        else:
+            e = int(rng.integers(1, t + 1))
+            pos = rng.choice(n, e, replace=False).tolist()
+            buf = torch.randint(0, 256, (n * L,), dtype=torch.uint8, device="cuda", generator=g)
+            jobs.append(afrs.Job.recover(n, t, buf, L, pos))
+    return jobs
+
+
+def _plain_call(afrs, codecs, j):
+    c = codecs.get((j.n, j.t))
+    if c is None:
+        c = codecs[(j.n, j.t)] = afrs.Codec(j.n, j.t)
+    if j.op == 0:
+        c.encode_parity(j.src, j.dst, j.shard_len)
+    else:
+        c.recover_erasure_shards(j.dst, None, j.shard_len, j.positions)
+
+
+def run_small(args):
+    import torch
+
+    from oracle import oracle
+
+    afrs = _pkg()
+    n, t, L = 64, 32, 1024
+    msg = oracle.random_bytes((n - t) * L, 42)
+    ref = np.zeros(t * L, np.uint8)
+    oracle.encode_systematic_sharded(n, t, msg, ref, L)
+    cw = np.concatenate([ref, msg])
+    pos = sorted(np.random.default_rng(42).choice(n, t, replace=False).tolist())
+    codec = afrs.Codec(n, t)
+    d_msg = torch.from_numpy(msg).cuda()
+    d_par = torch.zeros(t * L, dtype=torch.uint8, device="cuda")
+    rx = cw.copy()
+    for p in pos:
+        rx[p * L:(p + 1) * L] = 0
+    d_rx = torch.from_numpy(rx).cuda()
+    for _ in range(args.warmup):
+        codec.encode_parity(d_msg, d_par, L)
+        codec.recover_erasure_shards(d_rx, None, L, pos)
+    torch.cuda.synchronize()
+    assert (d_par.cpu().numpy() == ref).all() and (d_rx.cpu().numpy() == cw).all()
+    res = {}
+    for op in ("encode", "recover"):
+        a, b = _events()
+        a.record()
+        for _ in range(args.steps):
+            if op == "encode":
+                codec.encode_parity(d_msg, d_par, L)
+            else:
+                codec.recover_erasure_shards(d_rx, None, L, pos)
+        b.record()
+        torch.cuda.synchronize()
+        us = a.elapsed_time(b) * 1e3 / args.steps
+        res[op] = {"us_per_op": round(us, 2), "GB/s": round(n * L / us / 1e3, 2)}
+    cpu = {op: round(oracle.gfni_throughput(op, n, t, L, 2000, 1) / 1e9, 3) for op in ("encode", "recover")}
+    print(json.dumps({"workload": "small: n=64 k=32 t=32 L=1KiB, encode + recover 32 random erasures",
+                      "gpu": res, "cpu_gfni_1thread_GB/s": cpu, "bit_exact": True}), flush=True)
+
+
+def run_batched(args):
+    import torch
+
+    afrs = _pkg()
+    S = afrs.serving
+    jobs = _make_jobs(afrs, 4096, seed=7)
+    total = sum(j.nbytes for j in jobs)
+    arr = S.make_job_array(jobs)
+    ctx = afrs.Context.get(0)
+    lib = afrs.lib()
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        lib.afrs_batch_dev(ctx.handle, arr, len(jobs), stream.cuda_stream)
+    torch.cuda.synchronize()
+    reps = max(3, min(args.steps, 20))
+    a, b = _events()
+    a.record()
+    for _ in range(reps):
+        lib.afrs_batch_dev(ctx.handle, arr, len(jobs), stream.cuda_stream)
+    b.record()
+    torch.cuda.synchronize()
+    batched_ms = a.elapsed_time(b) / reps
+    codecs = {}
+    for j in jobs[:64]:
+        _plain_call(afrs, codecs, j)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record()
+    for j in jobs:
+        _plain_call(afrs, codecs, j)
+    b.record()
+    torch.cuda.synchronize()
+    plain_ms = a.elapsed_time(b)
+    wall_plain = time.perf_counter() - t0
+    out = {
+        "workload": "batched: 4096 codewords, n in {32,64,128,256}, t in {4,8,n/4,n/2}, L log-uniform 64B-16KiB, "
+                    "e in 1..t, 50% encode / 50% recover",
+        "bytes_per_batch": total,
+        "batched": {"ms": round(batched_ms, 3), "GB/s": round(total / batched_ms / 1e6, 2), "launches": 2},
+        "per_call": {"ms": round(plain_ms, 3), "GB/s": round(total / plain_ms / 1e6, 2),
+                     "host_wall_ms": round(wall_plain * 1e3, 3)},
+        "speedup": round(plain_ms / batched_ms, 2),
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_serving(args):
+    import torch
+
+    afrs = _pkg()
+    S = afrs.serving
+    pool = _make_jobs(afrs, 1200, seed=11, tail_frac=0.05)
+    rng = np.random.default_rng(5)
+
+    def build(count):
+        idx = rng.integers(0, len(pool), count)
+        return [S.Request(pool[i]) for i in idx]
+
+    def run(server_cls, reqs, arrivals, **kw):
+        srv = server_cls(**kw)
+        done, wall = S.serve_open_loop(srv, reqs, arrivals, timeout_s=120.0)
+        torch.cuda.synchronize()
+        lat = [r.latency * 1e3 for r in done]
+        p = S.percentiles(lat)
+        nbytes = sum(r.nbytes for r in done)
+        return {"p50_ms": round(p[50], 3), "p99_ms": round(p[99], 3), "p999_ms": round(p[99.9], 3),
+                "GB/s": round(nbytes / wall / 1e9, 2), "requests": len(done)}
+
+    # warm up both paths and every kernel shape in the pool
+    run(S.BatchServer, build(200), [0.0] * 200)
+    run(S.PlainServer, build(200), [0.0] * 200)
+    cap_reqs = build(600)
+    cap_b = run(S.BatchServer, cap_reqs, [0.0] * len(cap_reqs))
+    cap_p = run(S.PlainServer, build(600), [0.0] * 600)
+    mean_bytes = sum(j.nbytes for j in pool) / len(pool)
+    levels = []
+    for frac in (0.1, 0.25, 0.5, 0.75, 1.0, 1.2):
+        rate = frac * cap_b["GB/s"] * 1e9 / mean_bytes  # requests per second
+        count = int(min(1500, max(100, rate * 0.6)))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, count)).tolist()
+        row = {"offered_frac_of_batched_capacity": frac, "offered_GB/s": round(frac * cap_b["GB/s"], 2)}
+        row["batched"] = run(S.BatchServer, build(count), arrivals)
+        row["per_call"] = run(S.PlainServer, build(count), arrivals)
+        levels.append(row)
+    print(json.dumps({"workload": "serving: Poisson arrivals of config-3 requests + 5% n=256 k=192 1MiB-shard tail, "
+                                  "32 GiB admission cap",
+                      "capacity_GB/s": {"batched": cap_b["GB/s"], "per_call": cap_p["GB/s"]},
+                      "levels": levels}), flush=True)
+
+
+def run_large(args):
+    import torch
+
+    afrs = _pkg()
+    n, t, L = 256, 32, 4 << 20
+    k = n - t
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    cw = torch.empty(n * L, dtype=torch.uint8, device="cuda")
+    cw[t * L:] = torch.randint(0, 256, (k * L,), dtype=torch.uint8, device="cuda", generator=g)
+    codec = afrs.Codec(n, t)
+    codec.encode_parity(cw[t * L:], cw[: t * L], L)
+    torch.cuda.synchronize()
+    a, b = _events()
+    reps = 3
+    a.record()
+    for _ in range(reps):
+        codec.encode_parity(cw[t * L:], cw[: t * L], L)
+    b.record()
+    torch.cuda.synchronize()
+    enc_ms = a.elapsed_time(b) / reps
+    rng = np.random.default_rng(1)
+    patterns = {"a_in_message": sorted(rng.choice(np.arange(32, 256), 32, replace=False).tolist()),
+                "b_contiguous": list(range(100, 132))}
+    out = {"workload": "large: n=256 k=224 t=32 L=4MiB (1 GiB codeword)",
+           "encode": {"ms": round(enc_ms, 3), "GB/s": round(n * L / enc_ms / 1e6, 2)}}
+    rx = torch.empty_like(cw)
+    for name, pos in patterns.items():
+        times = []
+        ok = True
+        for _ in range(reps):
+            rx.copy_(cw)
+            for p in pos:
+                rx[p * L:(p + 1) * L].zero_()
+            a.record()
+            codec.recover_erasure_shards(rx, None, L, pos)
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+            ok = ok and bool(torch.equal(rx, cw))
+        ms = sorted(times)[len(times) // 2]
+        out[name] = {"positions": f"{pos[0]}..{pos[-1]}" if name.startswith("b") else "32 random in 32..255",
+                     "ms": round(ms, 3), "GB/s": round(n * L / ms / 1e6, 2), "round_trip_bit_exact": ok}
+    print(json.dumps(out), flush=True)
+
+
+def run(name, args):
+    return {"small": run_small, "batched": run_batched, "serving": run_serving, "large": run_large}[name](args)

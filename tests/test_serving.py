@@ -1,0 +1,86 @@
+"""Serving loop: continuous batching gives every request the same bytes as
+serving it alone, respects the device-memory admission cap, and reports
+latency percentiles."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+torch = pytest.importorskip("torch")
+
+
+def test_percentiles(afrs):
+    p = afrs.serving.percentiles(list(range(1, 1001)))
+    assert p[50] == 501 and p[99] == 990 and p[99.9] == 999
+    assert afrs.serving.percentiles([])[50] is None
+
+
+def _requests(afrs, count, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.choice([32, 64, 128, 256]))
+        t = int(rng.choice([4, 8, n // 4, n // 2]))
+        L = 64 * int(rng.integers(1, 40))
+        msg = oracle.random_bytes((n - t) * L, seed * 7919 + i)
+        par = np.zeros(t * L, np.uint8)
+        oracle.encode_systematic_sharded(n, t, msg, par, L)
+        if i % 2 == 0:
+            job = afrs.Job.encode(n, t, torch.from_numpy(msg).cuda(), torch.zeros(t * L, dtype=torch.uint8,
+                                                                                   device="cuda"), L)
+        else:
+            cw = np.concatenate([par, msg])
+            pos = rng.choice(n, int(rng.integers(1, t + 1)), replace=False).tolist()
+            for p in pos:
+                cw[p * L:(p + 1) * L] = 0
+            job = afrs.Job.recover(n, t, torch.from_numpy(cw).cuda(), L, pos)
+        out.append(job)
+    return out
+
+
+def _clone(afrs, j):
+    src = j.src.clone() if j.src is not None else None
+    return afrs.Job(j.op, j.n, j.t, src, j.dst.clone(), j.shard_len, j.positions)
+
+
+@pytest.mark.gpu
+def test_result_alone_equals_result_in_the_mix(afrs):
+    S = afrs.serving
+    jobs = _requests(afrs, 60, seed=4)
+    alone = [_clone(afrs, j) for j in jobs]
+    reqs = [S.Request(j) for j in jobs]
+    arrivals = [i * 2e-5 for i in range(len(reqs))]  # arrivals overlap running batches
+    server = S.BatchServer(streams=3, max_batch_bytes=1 << 20)
+    done, _ = S.serve_open_loop(server, reqs, arrivals)
+    torch.cuda.synchronize()
+    assert len(done) == len(reqs) and server.batches > 1
+    for j in alone:  # each request served alone, as a batch of one
+        afrs.run_batch([j])
+    torch.cuda.synchronize()
+    for r, a in zip(reqs, alone):
+        assert r.status == a.status
+        assert torch.equal(r.dst, a.dst)  # exact: integer arithmetic, no tolerance
+        assert r.latency >= 0
+
+
+@pytest.mark.gpu
+def test_admission_cap_and_plain_server(afrs):
+    S = afrs.serving
+    jobs = _requests(afrs, 30, seed=8)
+    plain_jobs = [_clone(afrs, j) for j in jobs]
+    reqs = [S.Request(j) for j in jobs]
+    cap = 3 * max(r.nbytes for r in reqs)
+    server = S.BatchServer(streams=4, hbm_cap=cap)
+    peak = 0
+    for r in reqs:
+        server.submit(r)
+    done = []
+    while len(done) < len(reqs):
+        done.extend(server.poll())
+        peak = max(peak, server.inflight_bytes)
+    assert peak <= cap
+    preqs = [S.Request(j) for j in plain_jobs]
+    pdone, _ = S.serve_open_loop(S.PlainServer(), preqs, [0.0] * len(preqs))
+    torch.cuda.synchronize()
+    for r, p in zip(reqs, preqs):
+        assert torch.equal(r.dst, p.dst)
