@@ -65,10 +65,16 @@ def percentiles(values, ps=(50, 99, 99.9)):
 class BatchServer:
     """Continuous batching: up to ``streams`` batches in flight, each holding
     at most ``max_batch_bytes`` of codewords, all in flight together at most
-    ``hbm_cap`` bytes (the admission cap on device memory)."""
+    ``hbm_cap`` bytes (the admission cap on device memory).
+
+    Requests of at least ``large_bytes`` are not batched: one such codeword
+    already fills the GPU, and the per-shape kernels of the per-call path run
+    it faster than the batched kernel's shape-generic code, so they go one at
+    a time to a stream of their own, under the same admission cap, and never
+    hold back the small requests' batches."""
 
     def __init__(self, device: int = 0, streams: int = 3, max_batch_bytes: int = 512 << 20,
-                 hbm_cap: int = 32 << 30):
+                 hbm_cap: int = 32 << 30, large_bytes: int = 16 << 20):
         import torch
 
         self.device = device
@@ -80,18 +86,39 @@ class BatchServer:
         self.hbm_cap = hbm_cap
         self.inflight_bytes = 0
         self.batches = 0
+        self.large_bytes = large_bytes
+        self.large = PlainServer(device, window=4)
 
     def submit(self, req: Request) -> None:
-        self.queue.append(req)
+        if req.nbytes >= self.large_bytes:
+            self.large.submit(req)
+        else:
+            self.queue.append(req)
 
     def pending(self) -> int:
-        return len(self.queue) + sum(len(b[1]) for b in self.busy if b is not None)
+        return len(self.queue) + sum(len(b[1]) for b in self.busy if b is not None) + self.large.pending()
+
+    def _poll_large(self) -> list:
+        # admission: a large request enters the per-call stream only while the cap allows
+        admit = []
+        while self.large.queue and (self.inflight_bytes + self.large.queue[0].nbytes <= self.hbm_cap
+                                    or self.inflight_bytes == 0):
+            r = self.large.queue.popleft()
+            self.inflight_bytes += r.nbytes
+            admit.append(r)
+        held = list(self.large.queue)
+        self.large.queue = collections.deque(admit)
+        finished = self.large.poll()
+        self.large.queue.extend(held)
+        for r in finished:
+            self.inflight_bytes -= r.nbytes
+        return finished
 
     def poll(self) -> list:
         """Retire finished batches, launch new ones; returns finished requests."""
         import torch
 
-        finished = []
+        finished = self._poll_large()
         now = time.perf_counter()
         for i, b in enumerate(self.busy):
             if b is not None and b[0].query():

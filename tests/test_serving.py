@@ -50,10 +50,12 @@ def test_result_alone_equals_result_in_the_mix(afrs):
     alone = [_clone(afrs, j) for j in jobs]
     reqs = [S.Request(j) for j in jobs]
     arrivals = [i * 2e-5 for i in range(len(reqs))]  # arrivals overlap running batches
-    server = S.BatchServer(streams=3, max_batch_bytes=1 << 20)
+    # requests of 200 KB and more take the per-call path inside the server
+    server = S.BatchServer(streams=3, max_batch_bytes=1 << 20, large_bytes=200_000)
     done, _ = S.serve_open_loop(server, reqs, arrivals)
     torch.cuda.synchronize()
     assert len(done) == len(reqs) and server.batches > 1
+    assert any(r.nbytes >= 200_000 for r in reqs) and any(r.nbytes < 200_000 for r in reqs)
     for j in alone:  # each request served alone, as a batch of one
         afrs.run_batch([j])
     torch.cuda.synchronize()
