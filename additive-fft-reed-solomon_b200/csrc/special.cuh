@@ -269,20 +269,91 @@ struct Batch {
 
 constexpr int kPhaseThreads = 128;
 
+// ---- per-thread staging of 16 rows in shared memory -----------------------
+// Slot (row i, half h) of the calling thread: 16 bytes at
+// st[(i * 2 + h) * kPhaseThreads + tid] (consecutive threads, consecutive
+// 16-byte words).  Rows are fetched with cp.async (all 32 copies in flight at
+// once), transposed to planes in a rolled loop (one copy of the transpose
+// code instead of 16), then read into registers for the unrolled transform.
+// 16 rows x 32 bytes x kPhaseThreads = 64 KiB per CTA.
+constexpr size_t kStageBytes = (size_t)16 * 32 * kPhaseThreads;
+
+__device__ __forceinline__ uint4* st4(uint32_t* st, int i, int h) {
+  return reinterpret_cast<uint4*>(st) + (i * 2 + h) * kPhaseThreads + threadIdx.x;
+}
+
+__device__ __forceinline__ void cp_async16(uint4* dst, const uint8_t* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+// Rows first_row + i (i < 16) of colword w, except those whose bit is set in
+// `skip` (staged as zero).  Runs and tails that are not 16-byte aligned and
+// in bounds take ordinary loads.
+__device__ __forceinline__ void stage_rows(uint32_t* st, const uint8_t* base, size_t first_row, size_t L, size_t w,
+                                           uint32_t skip) {
+  const size_t c = cw_col(w);
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      uint4* dst = st4(st, i, h);
+      if ((skip >> i) & 1) {
+        *dst = make_uint4(0, 0, 0, 0);
+        continue;
+      }
+      const size_t col = c + 512 * h;
+      const uint8_t* row = base + (first_row + i) * L;
+      if (col + 16 <= L && ((reinterpret_cast<uintptr_t>(row + col) & 15) == 0)) {
+        cp_async16(dst, row + col);
+      } else {
+        uint32_t x[4];
+        load16(row, col, L, x);
+        *dst = make_uint4(x[0], x[1], x[2], x[3]);
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+__device__ __forceinline__ void st_get(uint32_t* st, int i, uint32_t (&x)[8]) {
+  const uint4 a = *st4(st, i, 0), b = *st4(st, i, 1);
+  x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+  x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+__device__ __forceinline__ void st_put(uint32_t* st, int i, const uint32_t (&x)[8]) {
+  *st4(st, i, 0) = make_uint4(x[0], x[1], x[2], x[3]);
+  *st4(st, i, 1) = make_uint4(x[4], x[5], x[6], x[7]);
+}
+
+// Staged bytes of the 16 rows -> planes, in place (rolled).
+__device__ __forceinline__ void stage_to_planes(uint32_t* st, const ShiftMul& km) {
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) {
+    uint32_t x[8];
+    st_get(st, i, x);
+    transpose8f(x, km);
+    st_put(st, i, x);
+  }
+}
+
 // ---- encode, t >= 32 -------------------------------------------------------
 // E1: bottom IFFT of chunk c (message shards (c-1)t .. ct-1, coset omega_ct),
 // group g: variant v = (c - 1) * (t/16) + g = blockIdx.y.  Scratch row =
 // message row.
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kPhaseThreads) k_enc_p1(EncodeArgs a, Batch bt) {
+__global__ void __launch_bounds__(kPhaseThreads, 3) k_enc_p1(EncodeArgs a, Batch bt) {
   constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
+  extern __shared__ uint32_t stage[];
   const ShiftMul km = make_shift_mul();
   const int v = blockIdx.y, c = v / G + 1, g = v % G;
+  stage_rows(stage, a.msg, (size_t)(c - 1) * T + 16 * g, a.L, bt.cw0 + w, 0);
+  stage_to_planes(stage, km);
   uint32_t x[16][8];
 #pragma unroll
-  for (int i = 0; i < 16; i++) gload(a.msg, (size_t)(c - 1) * T + 16 * g + i, a.L, bt.cw0 + w, x[i], km);
+  for (int i = 0; i < 16; i++) st_get(stage, i, x[i]);
   dispatch<0, C * G - 1>(v, [&](auto vv) {
     constexpr int V = decltype(vv)::value;
     block_ifft<0, 4, V % G, omega_c((V / G + 1) * T), 16>(x);
@@ -332,8 +403,9 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt
 
 // E3: bottom FFT of group g = blockIdx.y and store of parity rows 16g..16g+15.
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kPhaseThreads) k_enc_p3(EncodeArgs a, Batch bt) {
+__global__ void __launch_bounds__(kPhaseThreads, 3) k_enc_p3(EncodeArgs a, Batch bt) {
   constexpr int T = 1 << LOGT, G = T / 16;
+  extern __shared__ uint32_t stage[];
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
   const ShiftMul km = make_shift_mul();
@@ -346,7 +418,13 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p3(EncodeArgs a, Batch bt
     block_fft<0, 4, GG, 0, 16>(x);
   });
 #pragma unroll
-  for (int i = 0; i < 16; i++) gstore(a.parity, 16 * g + i, a.L, bt.cw0 + w, x[i], km);
+  for (int i = 0; i < 16; i++) st_put(stage, i, x[i]);
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) {
+    uint32_t y[8];
+    st_get(stage, i, y);
+    gstore(a.parity, 16 * g + i, a.L, bt.cw0 + w, y, km);
+  }
 }
 
 // ---- recover ------------------------------------------------------------
@@ -403,40 +481,58 @@ __global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
 //   R1: y = lambda .* r on group g, c' = IFFT_bot  -> s1
 //   R2: rows {b + 16m}: u' = FFT_top((I + D_top) IFFT_top(c'))  -> s2
 //   R3: group g with erasures: FFT_bot(s2 + (I + D_bot) s1), Forney, store.
-// Per-thread staging for rows that get a runtime scale: the scale runs in a
-// rolled loop (one copy of its code), the stage hands the rows to the
-// unrolled transform.  16 rows x 8 planes x kPhaseThreads words.
-__device__ __forceinline__ uint32_t* stage_at(uint32_t* st, int i, int p) {
-  return st + (i * 8 + p) * kPhaseThreads + threadIdx.x;
+// Erasure locator of one recover call, computed once (one warp) into the
+// last kLocReserve bytes of the scratch: erased flags, log lambda, log 1/lambda'.
+constexpr size_t kLocReserve = 1024;
+
+template <int LOGN>
+__global__ void __launch_bounds__(32) k_rec_locator(RecoverArgs a, uint8_t* loc) {
+  __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
+  erasure_locator_warp(a, c_tab, s_er, s_lam, s_ilp);
+  __syncwarp();
+  for (int i = threadIdx.x; i < 256; i += 32) {
+    loc[i] = s_er[i];
+    loc[256 + i] = s_lam[i];
+    loc[512 + i] = s_ilp[i];
+  }
+}
+
+__device__ __forceinline__ void load_locator(const uint8_t* loc, uint8_t* s_er, uint8_t* s_lam, uint8_t* s_ilp) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(loc);
+  for (int i = threadIdx.x; i < 192; i += blockDim.x) {
+    const uint32_t v = src[i];
+    uint8_t* dst = i < 64 ? s_er + 4 * i : (i < 128 ? s_lam + 4 * (i - 64) : s_ilp + 4 * (i - 128));
+    *reinterpret_cast<uint32_t*>(dst) = v;
+  }
+  __syncthreads();
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(kPhaseThreads) k_rec_p1(RecoverArgs a, Batch bt) {
-  __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
+__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p1(RecoverArgs a, Batch bt, const uint8_t* loc) {
+  __shared__ __align__(16) uint8_t s_er[256], s_lam[256], s_ilp[256];
   extern __shared__ uint32_t stage[];
-  if (threadIdx.x < 32) erasure_locator_warp(a, c_tab, s_er, s_lam, s_ilp);
-  __syncthreads();
+  load_locator(loc, s_er, s_lam, s_ilp);
   constexpr int G = (1 << LOGN) / 16;
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
   const ShiftMul km = make_shift_mul();
   const int g = blockIdx.y;
-#pragma unroll 1
-  for (int i = 0; i < 16; i++) {
-    const int r = 16 * g + i;
-    uint32_t y[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (!s_er[r]) {
-      gload(a.rx, r, a.L, bt.cw0 + w, y, km);
-      scale_log(y, s_lam[r]);
-    }
+  uint32_t skip = 0;
 #pragma unroll
-    for (int p = 0; p < 8; p++) *stage_at(stage, i, p) = y[p];
+  for (int i = 0; i < 16; i++) skip |= (uint32_t)(s_er[16 * g + i] != 0) << i;
+  stage_rows(stage, a.rx, 16 * g, a.L, bt.cw0 + w, skip);
+#pragma unroll 1
+  for (int i = 0; i < 16; i++) {  // planes, lambda scale (rolled: one copy of the scale code)
+    if ((skip >> i) & 1) continue;
+    uint32_t y[8];
+    st_get(stage, i, y);
+    transpose8f(y, km);
+    scale_log(y, s_lam[16 * g + i]);
+    st_put(stage, i, y);
   }
   uint32_t x[16][8];
 #pragma unroll
-  for (int i = 0; i < 16; i++)
-#pragma unroll
-    for (int p = 0; p < 8; p++) x[i][p] = *stage_at(stage, i, p);
+  for (int i = 0; i < 16; i++) st_get(stage, i, x[i]);
   dispatch<0, G - 1>(g, [&](auto v) {
     constexpr int GG = decltype(v)::value;
     block_ifft<0, 4, GG, 0, 16>(x);
@@ -468,11 +564,10 @@ struct GroupList {
 };
 
 template <int LOGN>
-__global__ void __launch_bounds__(kPhaseThreads) k_rec_p3(RecoverArgs a, Batch bt, GroupList gl) {
-  __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
+__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p3(RecoverArgs a, Batch bt, GroupList gl, const uint8_t* loc) {
+  __shared__ __align__(16) uint8_t s_er[256], s_lam[256], s_ilp[256];
   extern __shared__ uint32_t stage[];
-  if (threadIdx.x < 32) erasure_locator_warp(a, c_tab, s_er, s_lam, s_ilp);
-  __syncthreads();
+  load_locator(loc, s_er, s_lam, s_ilp);
   constexpr int G = (1 << LOGN) / 16;
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
@@ -494,16 +589,13 @@ __global__ void __launch_bounds__(kPhaseThreads) k_rec_p3(RecoverArgs a, Batch b
     block_fft<0, 4, GG, 0, 16>(x);
   });
 #pragma unroll
-  for (int i = 0; i < 16; i++)
-#pragma unroll
-    for (int p = 0; p < 8; p++) *stage_at(stage, i, p) = x[i][p];
+  for (int i = 0; i < 16; i++) st_put(stage, i, x[i]);
 #pragma unroll 1
   for (int i = 0; i < 16; i++) {
     const int r = 16 * g + i;
     if (!s_er[r]) continue;
     uint32_t y[8];
-#pragma unroll
-    for (int p = 0; p < 8; p++) y[p] = *stage_at(stage, i, p);
+    st_get(stage, i, y);
     scale_log(y, s_ilp[r]);
     gstore(a.rx, r, a.L, bt.cw0 + w, y, km);
   }
@@ -512,7 +604,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_rec_p3(RecoverArgs a, Batch b
 // ---- launchers ------------------------------------------------------------
 
 // Scratch budget per phase batch: both buffers together stay well inside L2.
-constexpr size_t kScratchBudget = (size_t)48 << 20;
+constexpr size_t kScratchBudget = (size_t)128 << 20;
 
 // Colwords covering L bytes in the io.cuh layout (whole 1024-column slices).
 inline size_t total_colwords(size_t L) { return (L + 1023) / 1024 * 32; }
@@ -542,12 +634,17 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
     const size_t total_cw = total_colwords(a.L);
     const size_t bcw = batch_colwords(N - T, 1, sc.bytes, total_cw);
     if (bcw == 0) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaFuncSetAttribute(k_enc_p1<LOGN, LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kStageBytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_enc_p3<LOGN, LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+    if (e != cudaSuccess) return e;
     for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
       Batch bt{sc.ptr, nullptr, (total_cw - cw0 < bcw ? total_cw - cw0 : bcw), cw0};
       const unsigned gx = (unsigned)((bt.ncw + kPhaseThreads - 1) / kPhaseThreads);
-      k_enc_p1<LOGN, LOGT><<<dim3(gx, C * G), kPhaseThreads, 0, s>>>(a, bt);
+      k_enc_p1<LOGN, LOGT><<<dim3(gx, C * G), kPhaseThreads, kStageBytes, s>>>(a, bt);
       k_enc_p2<LOGN, LOGT><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_enc_p3<LOGN, LOGT><<<dim3(gx, G), kPhaseThreads, 0, s>>>(a, bt);
+      k_enc_p3<LOGN, LOGT><<<dim3(gx, G), kPhaseThreads, kStageBytes, s>>>(a, bt);
     }
     return cudaGetLastError();
   }
@@ -567,20 +664,23 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
     for (int g = 0; g < G; g++)
       if (has[g]) gl.g[gl.count++] = (uint8_t)g;
     const size_t total_cw = total_colwords(a.L);
-    const size_t bcw = batch_colwords(N, 2, sc.bytes, total_cw);
+    if (sc.bytes <= kLocReserve) return cudaErrorMemoryAllocation;
+    uint8_t* loc = reinterpret_cast<uint8_t*>(sc.ptr) + (sc.bytes - kLocReserve) / 256 * 256;
+    const size_t bcw = batch_colwords(N, 2, (size_t)(loc - reinterpret_cast<uint8_t*>(sc.ptr)), total_cw);
     if (bcw == 0) return cudaErrorMemoryAllocation;
-    constexpr size_t stage_bytes = (size_t)16 * 8 * kPhaseThreads * 4;
+    constexpr size_t stage_bytes = kStageBytes;
     cudaError_t e = cudaFuncSetAttribute(k_rec_p1<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_rec_p3<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
     if (e != cudaSuccess) return e;
+    k_rec_locator<LOGN><<<1, 32, 0, s>>>(a, loc);
     for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
       const size_t ncw = total_cw - cw0 < bcw ? total_cw - cw0 : bcw;
       Batch bt{sc.ptr, sc.ptr + (size_t)N * ncw * 8, ncw, cw0};
       const unsigned gx = (unsigned)((ncw + kPhaseThreads - 1) / kPhaseThreads);
-      k_rec_p1<LOGN><<<dim3(gx, G), kPhaseThreads, stage_bytes, s>>>(a, bt);
+      k_rec_p1<LOGN><<<dim3(gx, G), kPhaseThreads, stage_bytes, s>>>(a, bt, loc);
       k_rec_p2<LOGN><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_rec_p3<LOGN><<<dim3(gx, gl.count), kPhaseThreads, stage_bytes, s>>>(a, bt, gl);
+      k_rec_p3<LOGN><<<dim3(gx, gl.count), kPhaseThreads, stage_bytes, s>>>(a, bt, gl, loc);
     }
     return cudaGetLastError();
   }
@@ -591,7 +691,9 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
 inline size_t scratch_full_bytes_enc(int n, int t, size_t L) {
   return t >= 32 ? (size_t)(n - t) * total_colwords(L) * 32 : 0;
 }
-inline size_t scratch_full_bytes_rec(int n, size_t L) { return n >= 32 ? (size_t)2 * n * total_colwords(L) * 32 : 0; }
+inline size_t scratch_full_bytes_rec(int n, size_t L) {
+  return n >= 32 ? (size_t)2 * n * total_colwords(L) * 32 + kLocReserve : 0;
+}
 
 // Per-shape entry points, one translation unit each (special_enc_*.cu,
 // special_rec_*.cu) so that the build parallelises.

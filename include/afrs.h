@@ -67,7 +67,7 @@ int afrs_recover(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* received, size_
  * (a cudaStream_t; NULL = the legacy default stream).  Positions are read
  * from host memory during the call.  For t >= 32 (encode) and n >= 32
  * (recover) the kernels keep intermediate rows in a device scratch buffer
- * owned by the context: the first call of a size grows it (at most 48 MiB;
+ * owned by the context: the first call of a size grows it (at most 128 MiB;
  * longer shards are processed in column batches), and calls that share a
  * context are ordered on that buffer even when they use different streams. */
 int afrs_encode_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, const uint8_t* d_message,
@@ -124,10 +124,10 @@ int afrs_batch_dev(afrs_ctx* ctx, afrs_job* jobs, size_t count, void* stream);
  * serving loops that must never wait on the device-wide synchronisation an
  * allocation may take, and hosts that give the library a fixed memory
  * budget.  Same arguments and results as afrs_recover_dev, on the current
- * device, without a context.  Its scratch is a 32 MiB array of device
+ * device, without a context.  Its scratch is a 33 MiB array of device
  * memory compiled into the library (held by every GPU that loads it, until
  * the process exits); shards that need more (n * ceil(shard_len/1024) * 2 KiB
- * > 32 MiB for n >= 32, e.g. n = 256 with shard_len > 64 KiB) are refused
+ * + 1 KiB > 33 MiB for n >= 32, e.g. n = 256 with shard_len > 64 KiB) are refused
  * with AFRS_EINVAL and a message in afrs_last_error().  The first call on a
  * device looks up the array's device address (a set-up step), so make it
  * before any stream capture.  All calls share the one array: calls that
