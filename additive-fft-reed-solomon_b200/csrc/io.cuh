@@ -115,7 +115,13 @@ __device__ __forceinline__ void store_cw(uint8_t* row, size_t L, size_t w, const
 //            (rs/src/codec.rs:436-465 computes the same values directly).
 // Lane l owns indices 8l .. 8l+7.  Levels h < n only, so indices >= n
 // never mix into indices < n.
-__device__ __forceinline__ int mod255(int v) { return v % 255; }
+// v mod 255 for 0 <= v < 65536 without a division: 256 = 1 (mod 255), so
+// folding the high byte onto the low byte keeps the residue.
+__device__ __forceinline__ int mod255(int v) {
+  v = (v & 255) + (v >> 8);  // < 511
+  v = (v & 255) + (v >> 8);  // < 256
+  return v >= 255 ? v - 255 : v;
+}
 
 __device__ __forceinline__ void fwht_warp(int (&v)[8], int n, int lane) {
 #pragma unroll
