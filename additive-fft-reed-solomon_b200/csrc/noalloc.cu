@@ -20,10 +20,9 @@
 
 namespace {
 
-// 33 MiB: enough for one n = 256 codeword with 64 KiB shards (32 MiB of
-// intermediate rows plus the erasure-locator table).  Every GPU that loads
-// this library holds the array until the process exits.
-constexpr size_t kNoAllocScratchBytes = (size_t)33 << 20;
+// 32 MiB: enough for one n = 256 codeword with 64 KiB shards.  Every GPU
+// that loads this library holds the array until the process exits.
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;

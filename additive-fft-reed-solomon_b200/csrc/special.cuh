@@ -481,37 +481,56 @@ __global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
 //   R1: y = lambda .* r on group g, c' = IFFT_bot  -> s1
 //   R2: rows {b + 16m}: u' = FFT_top((I + D_top) IFFT_top(c'))  -> s2
 //   R3: group g with erasures: FFT_bot(s2 + (I + D_bot) s1), Forney, store.
-// Erasure locator of one recover call, computed once (one warp) into the
-// last kLocReserve bytes of the scratch: erased flags, log lambda, log 1/lambda'.
-constexpr size_t kLocReserve = 1024;
+// Erasure locator of one recover call, computed on the host by the launcher
+// and passed to the kernels as a parameter (constant bank): erased flags,
+// log lambda(omega_x) and log 1/lambda'(omega_x).  Same log-domain
+// Walsh-Hadamard computation as erasure_locator_warp (io.cuh), mod 255.
+struct LocTable {
+  uint8_t er[256], lam[256], ilp[256];
+};
 
-template <int LOGN>
-__global__ void __launch_bounds__(32) k_rec_locator(RecoverArgs a, uint8_t* loc) {
-  __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
-  erasure_locator_warp(a, c_tab, s_er, s_lam, s_ilp);
-  __syncwarp();
-  for (int i = threadIdx.x; i < 256; i += 32) {
-    loc[i] = s_er[i];
-    loc[256 + i] = s_lam[i];
-    loc[512 + i] = s_ilp[i];
+inline int host_mod255(int v) {
+  v %= 255;
+  return v < 0 ? v + 255 : v;
+}
+
+inline void host_fwht255(int* v, int n) {
+  for (int h = 1; h < n; h <<= 1)
+    for (int i = 0; i < n; i += 2 * h)
+      for (int j = i; j < i + h; j++) {
+        const int x = v[j], y = v[j + h];
+        v[j] = host_mod255(x + y);
+        v[j + h] = host_mod255(x - y);
+      }
+}
+
+inline void host_locator(const RecoverArgs& a, LocTable* t) {
+  const int n = a.n;
+  int ve[256] = {}, vl[256] = {};
+  *t = LocTable{};
+  for (int j = 0; j < a.e; j++) t->er[a.pos[j]] = 1;
+  for (int x = 0; x < n; x++) {
+    ve[x] = t->er[x];
+    vl[x] = x ? kField.log[kField.omega[x]] : 0;
+  }
+  host_fwht255(ve, n);
+  host_fwht255(vl, n);
+  for (int x = 0; x < n; x++) ve[x] = host_mod255(ve[x] * vl[x]);
+  host_fwht255(ve, n);
+  const int k = __builtin_ctz((unsigned)n);
+  const int ninv = (1 << (8 - k)) % 255;
+  for (int x = 0; x < n; x++) {
+    const int sv = host_mod255(ve[x] * ninv);
+    t->lam[x] = (uint8_t)sv;
+    t->ilp[x] = (uint8_t)host_mod255(255 - sv);
   }
 }
 
-__device__ __forceinline__ void load_locator(const uint8_t* loc, uint8_t* s_er, uint8_t* s_lam, uint8_t* s_ilp) {
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(loc);
-  for (int i = threadIdx.x; i < 192; i += blockDim.x) {
-    const uint32_t v = src[i];
-    uint8_t* dst = i < 64 ? s_er + 4 * i : (i < 128 ? s_lam + 4 * (i - 64) : s_ilp + 4 * (i - 128));
-    *reinterpret_cast<uint32_t*>(dst) = v;
-  }
-  __syncthreads();
-}
-
 template <int LOGN>
-__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p1(RecoverArgs a, Batch bt, const uint8_t* loc) {
-  __shared__ __align__(16) uint8_t s_er[256], s_lam[256], s_ilp[256];
+__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
+  const uint8_t* s_er = loc.er;
+  const uint8_t* s_lam = loc.lam;
   extern __shared__ uint32_t stage[];
-  load_locator(loc, s_er, s_lam, s_ilp);
   constexpr int G = (1 << LOGN) / 16;
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
@@ -564,10 +583,11 @@ struct GroupList {
 };
 
 template <int LOGN>
-__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p3(RecoverArgs a, Batch bt, GroupList gl, const uint8_t* loc) {
-  __shared__ __align__(16) uint8_t s_er[256], s_lam[256], s_ilp[256];
+__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p3(RecoverArgs a, Batch bt, GroupList gl,
+                                                             const __grid_constant__ LocTable loc) {
+  const uint8_t* s_er = loc.er;
+  const uint8_t* s_ilp = loc.ilp;
   extern __shared__ uint32_t stage[];
-  load_locator(loc, s_er, s_lam, s_ilp);
   constexpr int G = (1 << LOGN) / 16;
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
@@ -664,16 +684,15 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
     for (int g = 0; g < G; g++)
       if (has[g]) gl.g[gl.count++] = (uint8_t)g;
     const size_t total_cw = total_colwords(a.L);
-    if (sc.bytes <= kLocReserve) return cudaErrorMemoryAllocation;
-    uint8_t* loc = reinterpret_cast<uint8_t*>(sc.ptr) + (sc.bytes - kLocReserve) / 256 * 256;
-    const size_t bcw = batch_colwords(N, 2, (size_t)(loc - reinterpret_cast<uint8_t*>(sc.ptr)), total_cw);
+    LocTable loc;
+    host_locator(a, &loc);
+    const size_t bcw = batch_colwords(N, 2, sc.bytes, total_cw);
     if (bcw == 0) return cudaErrorMemoryAllocation;
     constexpr size_t stage_bytes = kStageBytes;
     cudaError_t e = cudaFuncSetAttribute(k_rec_p1<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_rec_p3<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
     if (e != cudaSuccess) return e;
-    k_rec_locator<LOGN><<<1, 32, 0, s>>>(a, loc);
     for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
       const size_t ncw = total_cw - cw0 < bcw ? total_cw - cw0 : bcw;
       Batch bt{sc.ptr, sc.ptr + (size_t)N * ncw * 8, ncw, cw0};
@@ -691,9 +710,7 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
 inline size_t scratch_full_bytes_enc(int n, int t, size_t L) {
   return t >= 32 ? (size_t)(n - t) * total_colwords(L) * 32 : 0;
 }
-inline size_t scratch_full_bytes_rec(int n, size_t L) {
-  return n >= 32 ? (size_t)2 * n * total_colwords(L) * 32 + kLocReserve : 0;
-}
+inline size_t scratch_full_bytes_rec(int n, size_t L) { return n >= 32 ? (size_t)2 * n * total_colwords(L) * 32 : 0; }
 
 // Per-shape entry points, one translation unit each (special_enc_*.cu,
 // special_rec_*.cu) so that the build parallelises.

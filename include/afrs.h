@@ -124,10 +124,10 @@ int afrs_batch_dev(afrs_ctx* ctx, afrs_job* jobs, size_t count, void* stream);
  * serving loops that must never wait on the device-wide synchronisation an
  * allocation may take, and hosts that give the library a fixed memory
  * budget.  Same arguments and results as afrs_recover_dev, on the current
- * device, without a context.  Its scratch is a 33 MiB array of device
+ * device, without a context.  Its scratch is a 32 MiB array of device
  * memory compiled into the library (held by every GPU that loads it, until
  * the process exits); shards that need more (n * ceil(shard_len/1024) * 2 KiB
- * + 1 KiB > 33 MiB for n >= 32, e.g. n = 256 with shard_len > 64 KiB) are refused
+ * > 32 MiB for n >= 32, e.g. n = 256 with shard_len > 64 KiB) are refused
  * with AFRS_EINVAL and a message in afrs_last_error().  The first call on a
  * device looks up the array's device address (a set-up step), so make it
  * before any stream capture.  All calls share the one array: calls that

@@ -58,7 +58,7 @@ def test_noalloc_matches_regular_entry_point_twice(afrs, n, t, L):
 
 @pytest.mark.gpu
 def test_noalloc_refuses_shards_beyond_its_scratch(afrs):
-    n, t, L = 256, 128, 68 * 1024  # needs 34 MiB + 1 KiB of scratch
+    n, t, L = 256, 128, 68 * 1024  # needs 34 MiB of scratch
     d = torch.zeros(n * L, dtype=torch.uint8, device="cuda")
     r = _noalloc(afrs, n, t, d, L, [0, 1])
     assert r == afrs._lib.AFRS_EINVAL
