@@ -338,30 +338,6 @@ __device__ __forceinline__ void stage_to_planes(uint32_t* st, const ShiftMul& km
 }
 
 // ---- encode, t >= 32 -------------------------------------------------------
-// E1: bottom IFFT of chunk c (message shards (c-1)t .. ct-1, coset omega_ct),
-// group g: variant v = (c - 1) * (t/16) + g = blockIdx.y.  Scratch row =
-// message row.
-template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kPhaseThreads, 3) k_enc_p1(EncodeArgs a, Batch bt) {
-  constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
-  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
-  if (w >= bt.ncw) return;
-  extern __shared__ uint32_t stage[];
-  const ShiftMul km = make_shift_mul();
-  const int v = blockIdx.y, c = v / G + 1, g = v % G;
-  stage_rows(stage, a.msg, (size_t)(c - 1) * T + 16 * g, a.L, bt.cw0 + w, 0);
-  stage_to_planes(stage, km);
-  uint32_t x[16][8];
-#pragma unroll
-  for (int i = 0; i < 16; i++) st_get(stage, i, x[i]);
-  dispatch<0, C * G - 1>(v, [&](auto vv) {
-    constexpr int V = decltype(vv)::value;
-    block_ifft<0, 4, V % G, omega_c((V / G + 1) * T), 16>(x);
-  });
-#pragma unroll
-  for (int i = 0; i < 16; i++) xstore(bt.s1, bt.ncw, (c - 1) * T + 16 * g + i, w, x[i]);
-}
-
 // E2: top levels for rows {b + 16 m} (b = blockIdx.y): IFFT top of every
 // chunk, accumulated, plus parity_in, then FFT top at 0; written to scratch
 // rows b + 16 m (chunk 1's rows, read above by this thread only).
@@ -401,29 +377,195 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt
   for (int m = 0; m < TR; m++) xstore(bt.s1, bt.ncw, b + 16 * m, w, acc[m]);
 }
 
-// E3: bottom FFT of group g = blockIdx.y and store of parity rows 16g..16g+15.
+
+// ---- bottom passes split over a warp pair -------------------------------
+// A 16-row bottom group (levels 0..3) is shared by two warps of a CTA: warp
+// h of a pair holds rows 16g + 8h + i (i < 8) of the same 32 colwords.  Levels
+// 0..2 run inside each warp (a warp-uniform compile-time variant of ~12
+// butterflies: small enough for the per-sub-partition instruction cache),
+// level 3 pairs row i of warp 0 with row i of warp 1 and goes through shared
+// memory.  Half the registers of a 16-row task, so more warps per SM.
+constexpr int kSplitThreads = 128;  // two warp pairs, 64 colwords
+constexpr size_t kStage8Bytes = (size_t)8 * 32 * kSplitThreads;
+
+__device__ __forceinline__ uint4* s8(uint32_t* st, int i, int hf, int tid) {
+  return reinterpret_cast<uint4*>(st) + (i * 2 + hf) * kSplitThreads + tid;
+}
+__device__ __forceinline__ void s8_get(uint32_t* st, int i, int tid, uint32_t (&x)[8]) {
+  const uint4 a = *s8(st, i, 0, tid), b = *s8(st, i, 1, tid);
+  x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+  x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+__device__ __forceinline__ void s8_put(uint32_t* st, int i, int tid, const uint32_t (&x)[8]) {
+  *s8(st, i, 0, tid) = make_uint4(x[0], x[1], x[2], x[3]);
+  *s8(st, i, 1, tid) = make_uint4(x[4], x[5], x[6], x[7]);
+}
+
+// Rows first_row + i (i < 8) of colword w into the calling thread's slots
+// (cp.async where 16-byte aligned and in bounds); bit i of skip stages zero.
+__device__ __forceinline__ void stage8(uint32_t* st, const uint8_t* base, size_t first_row, size_t L, size_t w,
+                                       uint32_t skip) {
+  const size_t c = cw_col(w);
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+#pragma unroll
+    for (int hf = 0; hf < 2; hf++) {
+      uint4* dst = s8(st, i, hf, tid);
+      if ((skip >> i) & 1) {
+        *dst = make_uint4(0, 0, 0, 0);
+        continue;
+      }
+      const size_t col = c + 512 * hf;
+      const uint8_t* row = base + (first_row + i) * L;
+      if (col + 16 <= L && ((reinterpret_cast<uintptr_t>(row + col) & 15) == 0)) {
+        cp_async16(dst, row + col);
+      } else {
+        uint32_t x[4];
+        load16(row, col, L, x);
+        *dst = make_uint4(x[0], x[1], x[2], x[3]);
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Level 3 of an IFFT over the pair: (g0, g1) = (row i of warp 0, row i of
+// warp 1) -> (g0 + T*(g0 + g1), g0 + g1).  The rows are exchanged through the
+// stage; ends with a barrier after which the stage may be reused.
+template <int TW>
+__device__ __forceinline__ void pair_ifft_level3(uint32_t* st, uint32_t (&x)[8][8], int h) {
+  const int tid = threadIdx.x;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    uint32_t y[8];
+    s8_get(st, i, tid ^ 32, y);
+    if (h == 0) {
+      uint32_t d[8];
+#pragma unroll
+      for (int p = 0; p < 8; p++) d[p] = x[i][p] ^ y[p];
+      if constexpr (TW != 0) mul_xor_c<static_cast<uint8_t>(TW)>(x[i], d);
+    } else {
+#pragma unroll
+      for (int p = 0; p < 8; p++) x[i][p] ^= y[p];
+    }
+  }
+  __syncthreads();
+}
+
+// Level 3 of an FFT over the pair: (a, b) -> (a + T*b, a + (T+1)*b).
+template <int TW>
+__device__ __forceinline__ void pair_fft_level3(uint32_t* st, uint32_t (&x)[8][8], int h) {
+  const int tid = threadIdx.x;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    uint32_t y[8];
+    s8_get(st, i, tid ^ 32, y);
+    if (h == 0) {
+      if constexpr (TW != 0) mul_xor_c<static_cast<uint8_t>(TW)>(x[i], y);
+    } else {
+      uint32_t m[8];
+#pragma unroll
+      for (int p = 0; p < 8; p++) m[p] = y[p] ^ x[i][p];
+      if constexpr (TW != 0) mul_xor_c<static_cast<uint8_t>(TW)>(m, x[i]);
+#pragma unroll
+      for (int p = 0; p < 8; p++) x[i][p] = m[p];
+    }
+  }
+  __syncthreads();
+}
+
+struct PairPos {
+  int h;
+  size_t w;
+  bool active;
+};
+__device__ __forceinline__ PairPos pair_pos(size_t ncw) {
+  const int warp = threadIdx.x >> 5;
+  PairPos q;
+  q.h = warp & 1;
+  q.w = (size_t)blockIdx.x * 64 + (warp >> 1) * 32 + (threadIdx.x & 31);
+  q.active = q.w < ncw;
+  return q;
+}
+
+// E1 (split): bottom IFFT of chunk c, group g; blockIdx.y = (c - 1) * (t/16) + g.
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kPhaseThreads, 3) k_enc_p3(EncodeArgs a, Batch bt) {
+__global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt) {
+  constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
+  extern __shared__ uint32_t st[];
+  const PairPos q = pair_pos(bt.ncw);
+  const ShiftMul km = make_shift_mul();
+  const int v = blockIdx.y, c = v / G + 1, g = v % G;
+  const size_t row0 = (size_t)(c - 1) * T + 16 * g + 8 * q.h;
+  uint32_t x[8][8];
+  zero_rows(x);
+  if (q.active) {
+    stage8(st, a.msg, row0, a.L, bt.cw0 + q.w, 0);
+#pragma unroll 1
+    for (int i = 0; i < 8; i++) {
+      uint32_t y[8];
+      s8_get(st, i, threadIdx.x, y);
+      transpose8f(y, km);
+      s8_put(st, i, threadIdx.x, y);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) s8_get(st, i, threadIdx.x, x[i]);
+  }
+  dispatch<0, 2 * C * G - 1>(2 * v + q.h, [&](auto vv) {
+    constexpr int VV = decltype(vv)::value, V = VV / 2, H = VV % 2;
+    block_ifft<0, 3, 2 * (V % G) + H, omega_c((V / G + 1) * T), 8>(x);
+  });
+  dispatch<0, C * G - 1>(v, [&](auto vv) {
+    constexpr int V = decltype(vv)::value;
+    pair_ifft_level3<twiddle_c(3, omega_c((V / G + 1) * T), 16 * (V % G))>(st, x, q.h);
+  });
+  if (q.active) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) xstore(bt.s1, bt.ncw, (int)row0 + i, q.w, x[i]);
+  }
+}
+
+// E3 (split): bottom FFT of group g = blockIdx.y, store of parity rows.
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt) {
   constexpr int T = 1 << LOGT, G = T / 16;
-  extern __shared__ uint32_t stage[];
-  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
-  if (w >= bt.ncw) return;
+  extern __shared__ uint32_t st[];
+  const PairPos q = pair_pos(bt.ncw);
   const ShiftMul km = make_shift_mul();
   const int g = blockIdx.y;
-  uint32_t x[16][8];
+  const int row0 = 16 * g + 8 * q.h;
+  uint32_t x[8][8];
+  zero_rows(x);
+  if (q.active) {
 #pragma unroll
-  for (int i = 0; i < 16; i++) xload(bt.s1, bt.ncw, 16 * g + i, w, x[i]);
-  dispatch<0, G - 1>(g, [&](auto v) {
-    constexpr int GG = decltype(v)::value;
-    block_fft<0, 4, GG, 0, 16>(x);
+    for (int i = 0; i < 8; i++) xload(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
+  }
+  dispatch<0, G - 1>(g, [&](auto vv) {
+    constexpr int GG = decltype(vv)::value;
+    pair_fft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
   });
+  dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
+    constexpr int VV = decltype(vv)::value;
+    block_fft<0, 3, VV, 0, 8>(x);
+  });
+  if (q.active) {
 #pragma unroll
-  for (int i = 0; i < 16; i++) st_put(stage, i, x[i]);
+    for (int i = 0; i < 8; i++) s8_put(st, i, threadIdx.x, x[i]);
 #pragma unroll 1
-  for (int i = 0; i < 16; i++) {
-    uint32_t y[8];
-    st_get(stage, i, y);
-    gstore(a.parity, 16 * g + i, a.L, bt.cw0 + w, y, km);
+    for (int i = 0; i < 8; i++) {
+      uint32_t y[8];
+      s8_get(st, i, threadIdx.x, y);
+      gstore(a.parity, row0 + i, a.L, bt.cw0 + q.w, y, km);
+    }
   }
 }
 
@@ -527,40 +669,6 @@ inline void host_locator(const RecoverArgs& a, LocTable* t) {
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
-  const uint8_t* s_er = loc.er;
-  const uint8_t* s_lam = loc.lam;
-  extern __shared__ uint32_t stage[];
-  constexpr int G = (1 << LOGN) / 16;
-  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
-  if (w >= bt.ncw) return;
-  const ShiftMul km = make_shift_mul();
-  const int g = blockIdx.y;
-  uint32_t skip = 0;
-#pragma unroll
-  for (int i = 0; i < 16; i++) skip |= (uint32_t)(s_er[16 * g + i] != 0) << i;
-  stage_rows(stage, a.rx, 16 * g, a.L, bt.cw0 + w, skip);
-#pragma unroll 1
-  for (int i = 0; i < 16; i++) {  // planes, lambda scale (rolled: one copy of the scale code)
-    if ((skip >> i) & 1) continue;
-    uint32_t y[8];
-    st_get(stage, i, y);
-    transpose8f(y, km);
-    scale_log(y, s_lam[16 * g + i]);
-    st_put(stage, i, y);
-  }
-  uint32_t x[16][8];
-#pragma unroll
-  for (int i = 0; i < 16; i++) st_get(stage, i, x[i]);
-  dispatch<0, G - 1>(g, [&](auto v) {
-    constexpr int GG = decltype(v)::value;
-    block_ifft<0, 4, GG, 0, 16>(x);
-  });
-#pragma unroll
-  for (int i = 0; i < 16; i++) xstore(bt.s1, bt.ncw, 16 * g + i, w, x[i]);
-}
-
-template <int LOGN>
 __global__ void __launch_bounds__(kPhaseThreads) k_rec_p2(RecoverArgs a, Batch bt) {
   constexpr int TL = LOGN - 4, TR = 1 << TL;
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
@@ -582,42 +690,110 @@ struct GroupList {
   uint8_t g[16];
 };
 
+
+// R1 (split): lambda-scale + bottom IFFT of group g = blockIdx.y.
 template <int LOGN>
-__global__ void __launch_bounds__(kPhaseThreads, 3) k_rec_p3(RecoverArgs a, Batch bt, GroupList gl,
-                                                             const __grid_constant__ LocTable loc) {
-  const uint8_t* s_er = loc.er;
-  const uint8_t* s_ilp = loc.ilp;
-  extern __shared__ uint32_t stage[];
+__global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
   constexpr int G = (1 << LOGN) / 16;
-  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
-  if (w >= bt.ncw) return;
+  extern __shared__ uint32_t st[];
+  const PairPos q = pair_pos(bt.ncw);
+  const ShiftMul km = make_shift_mul();
+  const int g = blockIdx.y;
+  const int row0 = 16 * g + 8 * q.h;
+  uint32_t x[8][8];
+  zero_rows(x);
+  if (q.active) {
+    uint32_t skip = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) skip |= (uint32_t)(loc.er[row0 + i] != 0) << i;
+    stage8(st, a.rx, row0, a.L, bt.cw0 + q.w, skip);
+#pragma unroll 1
+    for (int i = 0; i < 8; i++) {
+      if ((skip >> i) & 1) continue;
+      uint32_t y[8];
+      s8_get(st, i, threadIdx.x, y);
+      transpose8f(y, km);
+      scale_log(y, loc.lam[row0 + i]);
+      s8_put(st, i, threadIdx.x, y);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) s8_get(st, i, threadIdx.x, x[i]);
+  }
+  dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
+    constexpr int VV = decltype(vv)::value;
+    block_ifft<0, 3, VV, 0, 8>(x);
+  });
+  dispatch<0, G - 1>(g, [&](auto vv) {
+    constexpr int GG = decltype(vv)::value;
+    pair_ifft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
+  });
+  if (q.active) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) xstore(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
+  }
+}
+
+// R3 (split): x = s2 + (I + D_bot) s1 on group g, bottom FFT, Forney, store
+// the erased rows.  (I + D_bot) = (I + D_0..2) inside each warp plus, for
+// warp 0, the bit-3 term: row m gets original row m + 8 of warp 1.
+template <int LOGN>
+__global__ void __launch_bounds__(kSplitThreads) k_rec_b3(RecoverArgs a, Batch bt, GroupList gl,
+                                                           const __grid_constant__ LocTable loc) {
+  constexpr int G = (1 << LOGN) / 16;
+  extern __shared__ uint32_t st[];
+  const PairPos q = pair_pos(bt.ncw);
   const ShiftMul km = make_shift_mul();
   const int g = gl.g[blockIdx.y];
-  uint32_t x[16][8];
+  const int row0 = 16 * g + 8 * q.h;
+  const int tid = threadIdx.x;
+  uint32_t x[8][8];
+  zero_rows(x);
+  if (q.active) {
 #pragma unroll
-  for (int i = 0; i < 16; i++) xload(bt.s1, bt.ncw, 16 * g + i, w, x[i]);
-  one_plus_derivative<16>(x);
-#pragma unroll
-  for (int i = 0; i < 16; i++) {
-    uint32_t q[8];
-    xload(bt.s2, bt.ncw, 16 * g + i, w, q);
-#pragma unroll
-    for (int p = 0; p < 8; p++) x[i][p] ^= q[p];
+    for (int i = 0; i < 8; i++) xload(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
   }
-  dispatch<0, G - 1>(g, [&](auto v) {
-    constexpr int GG = decltype(v)::value;
-    block_fft<0, 4, GG, 0, 16>(x);
-  });
 #pragma unroll
-  for (int i = 0; i < 16; i++) st_put(stage, i, x[i]);
+  for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);  // original c' for the partner
+  __syncthreads();
+  one_plus_derivative<8>(x);
+  if (q.h == 0) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      uint32_t y[8];
+      s8_get(st, i, tid ^ 32, y);
+#pragma unroll
+      for (int p = 0; p < 8; p++) x[i][p] ^= y[p];
+    }
+  }
+  if (q.active) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      uint32_t u[8];
+      xload(bt.s2, bt.ncw, row0 + i, q.w, u);
+#pragma unroll
+      for (int p = 0; p < 8; p++) x[i][p] ^= u[p];
+    }
+  }
+  dispatch<0, G - 1>(g, [&](auto vv) {
+    constexpr int GG = decltype(vv)::value;
+    pair_fft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
+  });
+  dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
+    constexpr int VV = decltype(vv)::value;
+    block_fft<0, 3, VV, 0, 8>(x);
+  });
+  if (q.active) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);
 #pragma unroll 1
-  for (int i = 0; i < 16; i++) {
-    const int r = 16 * g + i;
-    if (!s_er[r]) continue;
-    uint32_t y[8];
-    st_get(stage, i, y);
-    scale_log(y, s_ilp[r]);
-    gstore(a.rx, r, a.L, bt.cw0 + w, y, km);
+    for (int i = 0; i < 8; i++) {
+      const int r = row0 + i;
+      if (!loc.er[r]) continue;
+      uint32_t y[8];
+      s8_get(st, i, tid, y);
+      scale_log(y, loc.ilp[r]);
+      gstore(a.rx, r, a.L, bt.cw0 + q.w, y, km);
+    }
   }
 }
 
@@ -654,17 +830,13 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
     const size_t total_cw = total_colwords(a.L);
     const size_t bcw = batch_colwords(N - T, 1, sc.bytes, total_cw);
     if (bcw == 0) return cudaErrorMemoryAllocation;
-    cudaError_t e = cudaFuncSetAttribute(k_enc_p1<LOGN, LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kStageBytes);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_enc_p3<LOGN, LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
-    if (e != cudaSuccess) return e;
     for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
       Batch bt{sc.ptr, nullptr, (total_cw - cw0 < bcw ? total_cw - cw0 : bcw), cw0};
       const unsigned gx = (unsigned)((bt.ncw + kPhaseThreads - 1) / kPhaseThreads);
-      k_enc_p1<LOGN, LOGT><<<dim3(gx, C * G), kPhaseThreads, kStageBytes, s>>>(a, bt);
+      const unsigned gs = (unsigned)((bt.ncw + 63) / 64);
+      k_enc_b1<LOGN, LOGT><<<dim3(gs, C * G), kSplitThreads, kStage8Bytes, s>>>(a, bt);
       k_enc_p2<LOGN, LOGT><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_enc_p3<LOGN, LOGT><<<dim3(gx, G), kPhaseThreads, kStageBytes, s>>>(a, bt);
+      k_enc_b3<LOGN, LOGT><<<dim3(gs, G), kSplitThreads, kStage8Bytes, s>>>(a, bt);
     }
     return cudaGetLastError();
   }
@@ -688,18 +860,15 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
     host_locator(a, &loc);
     const size_t bcw = batch_colwords(N, 2, sc.bytes, total_cw);
     if (bcw == 0) return cudaErrorMemoryAllocation;
-    constexpr size_t stage_bytes = kStageBytes;
-    cudaError_t e = cudaFuncSetAttribute(k_rec_p1<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_rec_p3<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes);
-    if (e != cudaSuccess) return e;
+
     for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
       const size_t ncw = total_cw - cw0 < bcw ? total_cw - cw0 : bcw;
       Batch bt{sc.ptr, sc.ptr + (size_t)N * ncw * 8, ncw, cw0};
       const unsigned gx = (unsigned)((ncw + kPhaseThreads - 1) / kPhaseThreads);
-      k_rec_p1<LOGN><<<dim3(gx, G), kPhaseThreads, stage_bytes, s>>>(a, bt, loc);
+      const unsigned gs = (unsigned)((ncw + 63) / 64);
+      k_rec_b1<LOGN><<<dim3(gs, G), kSplitThreads, kStage8Bytes, s>>>(a, bt, loc);
       k_rec_p2<LOGN><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_rec_p3<LOGN><<<dim3(gx, gl.count), kPhaseThreads, stage_bytes, s>>>(a, bt, gl, loc);
+      k_rec_b3<LOGN><<<dim3(gs, gl.count), kSplitThreads, kStage8Bytes, s>>>(a, bt, gl, loc);
     }
     return cudaGetLastError();
   }
