@@ -37,11 +37,14 @@ SIGNATURES = {
     "afrs_ctx_destroy": (None, [ctypes.c_void_p]),
     "afrs_last_error": (ctypes.c_char_p, []),
     "afrs_version": (ctypes.c_char_p, []),
+    "afrs_kernel_launches": (ctypes.c_uint64, []),
     "afrs_encode": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _u8p, _sz, ctypes.c_int]),
     "afrs_recover": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, _u8p, _sz]),
     "afrs_encode_dev": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _u8p, _sz, ctypes.c_int, ctypes.c_void_p]),
     "afrs_recover_dev": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, _u8p, _sz, ctypes.c_void_p]),
     "afrs_recompute_data_from_parity_dev": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, ctypes.c_void_p]),
+    "afrs_syndrome_dev": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, _u8p, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
     "afrs_fft_sharded_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _sz, _u32, ctypes.c_uint8, ctypes.c_void_p]),
     "afrs_ifft_sharded_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _sz, _u32, ctypes.c_uint8, ctypes.c_void_p]),
     "afrs_scale_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _u8p, _sz, ctypes.c_uint8, ctypes.c_void_p]),

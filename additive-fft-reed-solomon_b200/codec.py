@@ -166,6 +166,28 @@ class Codec:
                                                               shard_len, _stream(received)),
                "recompute_data_from_parity")
 
+    def syndrome_sharded(self, received, shard_len: int, syndrome=None):
+        """Sharded Codec::compute_syndrome_scalar (codec.rs:269-301) of a uint8
+        CUDA tensor of n shards: returns (syndrome, nonzero) where syndrome is a
+        t*shard_len CUDA tensor (``syndrome`` if given) and nonzero a one-element
+        int64 CUDA tensor counting its nonzero bytes (0 iff a codeword)."""
+        import torch
+
+        self._sizes(shard_len, received=received)
+        if syndrome is None:
+            syndrome = torch.empty(self.t * shard_len, dtype=torch.uint8, device=received.device)
+        self._sizes(shard_len, parity=syndrome)
+        nz = torch.zeros(1, dtype=torch.int64, device=received.device)
+        _check(_lib.lib().afrs_syndrome_dev(self.ctx.handle, self.n, self.t, _dev_ptr(received), shard_len,
+                                            _dev_ptr(syndrome), nz.data_ptr(), _stream(received)),
+               "syndrome_sharded")
+        return syndrome, nz
+
+    def is_codeword(self, received, shard_len: int) -> bool:
+        """True iff the n shards of ``received`` (CUDA tensor) form a codeword."""
+        _, nz = self.syndrome_sharded(received, shard_len)
+        return int(nz.item()) == 0
+
 
 def fft_sharded(shards, shard_len: int, k: int, beta: int, device: int = 0) -> None:
     """Kernel::fft_sharded (rs/src/kernel/mod.rs:8-14) on a uint8 CUDA tensor."""

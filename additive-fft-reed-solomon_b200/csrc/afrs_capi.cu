@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -143,11 +144,15 @@ int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
 
 namespace afrs {
 void set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+std::atomic<uint64_t> g_launches{0};
+void count_launches(unsigned k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 }  // namespace afrs
 
 extern "C" {
 
 const char* afrs_last_error(void) { return g_err; }
+
+uint64_t afrs_kernel_launches(void) { return afrs::g_launches.load(std::memory_order_relaxed); }
 
 const char* afrs_version(void) { return "afrs_b200 0.1 sm_100a (bit-sliced GF(2^8) additive FFT)"; }
 
@@ -324,6 +329,37 @@ static int transform_dev(afrs_ctx* c, uint8_t* d, size_t L, uint32_t k, uint8_t 
   DeviceGuard g(c->device);
   cudaError_t e = afrs::launch_transform_generic(d, L, (int)k, beta, inverse, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "transform launch");
+}
+
+// Syndrome (codec.rs:269-301, sharded): XOR_i IFFT_t(chunk i, omega_it) =
+// IFFT_t(parity) + acc with acc = XOR_{i>=1} IFFT_t(chunk i, omega_it), and
+// the encoder gives E = FFT_t(acc), so the syndrome is IFFT_t(parity + E, 0):
+// one encode (the fast kernels), one XOR pass and one t-point IFFT.
+int afrs_syndrome_dev(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* d_received, size_t L, uint8_t* d_syndrome,
+                      unsigned long long* d_nonzero, void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  int r = check_nt(n, t);
+  if (r) return r;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DeviceGuard g(c->device);
+  cudaError_t e;
+  if (d_nonzero && (e = cudaMemsetAsync(d_nonzero, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+    return cuda_fail(e, "syndrome count reset");
+  if (L == 0) return AFRS_OK;
+  if (!d_received || !d_syndrome) return fail(AFRS_EINVAL, "NULL buffer");
+  const size_t pb = (size_t)t * L;
+  if (d_syndrome < d_received + (size_t)n * L && d_received < d_syndrome + pb)
+    return fail(AFRS_EINVAL, "d_syndrome overlaps d_received");
+  afrs::EncodeArgs a{d_received + pb, d_syndrome, L, (int)n, (int)t, 0};
+  if ((r = launch_encode(c, a, s))) return r;
+  if ((e = afrs::launch_xor_into(d_syndrome, d_received, pb, s)) != cudaSuccess) return cuda_fail(e, "syndrome xor");
+  int k = 0;
+  while ((1u << k) < t) k++;
+  if (k > 0 && (e = afrs::launch_transform_generic(d_syndrome, L, k, 0, true, s)) != cudaSuccess)
+    return cuda_fail(e, "syndrome ifft");
+  if (d_nonzero && (e = afrs::launch_count_nonzero(d_syndrome, pb, d_nonzero, s)) != cudaSuccess)
+    return cuda_fail(e, "syndrome count");
+  return AFRS_OK;
 }
 
 int afrs_fft_sharded_dev(afrs_ctx* c, uint8_t* d, size_t L, uint32_t k, uint8_t beta, void* stream) {

@@ -56,6 +56,9 @@ cudaError_t launch_transform_generic(uint8_t* shards, size_t L, int k, uint8_t b
                                      cudaStream_t s);
 cudaError_t launch_recompute_generic(uint8_t* rx, size_t L, int t, cudaStream_t s);
 cudaError_t launch_scale(const uint8_t* src, uint8_t* dst, size_t len, uint8_t c, cudaStream_t s);
+// dst ^= src; *count += nonzero bytes of src (byte streams, any alignment).
+cudaError_t launch_xor_into(uint8_t* dst, const uint8_t* src, size_t len, cudaStream_t s);
+cudaError_t launch_count_nonzero(const uint8_t* src, size_t len, unsigned long long* count, cudaStream_t s);
 
 // Device scratch for the phase kernels (bit-sliced intermediate rows).
 struct ScratchArena {
@@ -73,6 +76,9 @@ cudaError_t launch_recover_special(const RecoverArgs& a, const ScratchArena& sc,
 size_t scratch_bytes_encode(int n, int t, size_t L);
 // Sets the calling thread's afrs_last_error() message.
 void set_last_error(const char* msg);
+// Adds k to the process-wide count of kernels this library has launched
+// (read back with afrs_kernel_launches()).
+void count_launches(unsigned k);
 size_t scratch_bytes_recover(int n, size_t L);
 
 }  // namespace afrs

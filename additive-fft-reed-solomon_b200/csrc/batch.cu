@@ -78,6 +78,7 @@ cudaError_t launch_batch(const BatchLaunch& b, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   if (b.nrec > 0) {
     k_batch_locator<<<b.nrec, kThreads, 0, s>>>(b.jobs, b.rec_jobs, b.pos_tab, b.loc_tab);
+    count_launches(1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (b.ntasks == 0) return cudaSuccess;
@@ -92,6 +93,7 @@ cudaError_t launch_batch(const BatchLaunch& b, cudaStream_t s) {
   size_t grid = (size_t)sms * (size_t)std::max(per_sm, 1);
   if (grid > (size_t)b.ntasks) grid = (size_t)b.ntasks;
   k_batch<<<(unsigned)grid, kThreads, smem, s>>>(b.jobs, b.tasks, b.ntasks, b.counter, b.pos_tab, b.loc_tab);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -89,6 +89,54 @@ cudaError_t set_smem(const void* fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// dst ^= src over len bytes.
+__global__ void k_xor_into(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, size_t len) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool vec = ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15) == 0;
+  size_t done = 0;
+  if (vec) {
+    const size_t nv = len / 16;
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    const uint4* q = reinterpret_cast<const uint4*>(src);
+    for (size_t v = i; v < nv; v += stride) {
+      uint4 a = d[v];
+      const uint4 b = q[v];
+      a.x ^= b.x;
+      a.y ^= b.y;
+      a.z ^= b.z;
+      a.w ^= b.w;
+      d[v] = a;
+    }
+    done = nv * 16;
+  }
+  for (size_t b = done + i; b < len; b += stride) dst[b] ^= src[b];
+}
+
+// *count += number of nonzero bytes in src[0, len).
+__global__ void k_count_nonzero(const uint8_t* __restrict__ src, size_t len, unsigned long long* count) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned c = 0;
+  size_t done = 0;
+  if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+    const size_t nv = len / 16;
+    const uint4* q = reinterpret_cast<const uint4*>(src);
+    for (size_t v = i; v < nv; v += stride) {
+      const uint4 b = q[v];
+      const uint32_t w[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) c += ((w[k] >> (8 * j)) & 0xFF) != 0;
+    }
+    done = nv * 16;
+  }
+  for (size_t b = done + i; b < len; b += stride) c += src[b] != 0;
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
 }  // namespace
 
 cudaError_t launch_encode_generic(const EncodeArgs& a, cudaStream_t s) {
@@ -97,6 +145,7 @@ cudaError_t launch_encode_generic(const EncodeArgs& a, cudaStream_t s) {
   cudaError_t err = set_smem((const void*)k_encode_generic, smem);
   if (err != cudaSuccess) return err;
   k_encode_generic<<<(unsigned)slices(a.L), kThreads, smem, s>>>(a);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -105,6 +154,7 @@ cudaError_t launch_recover_generic(const RecoverArgs& a, cudaStream_t s) {
   cudaError_t err = set_smem((const void*)k_recover_generic, smem);
   if (err != cudaSuccess) return err;
   k_recover_generic<<<(unsigned)slices(a.L), kThreads, smem, s>>>(a);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -114,6 +164,7 @@ cudaError_t launch_transform_generic(uint8_t* shards, size_t L, int k, uint8_t b
   cudaError_t err = set_smem((const void*)k_transform_generic, smem);
   if (err != cudaSuccess) return err;
   k_transform_generic<<<(unsigned)slices(L), kThreads, smem, s>>>(shards, L, k, beta, inverse);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -122,6 +173,7 @@ cudaError_t launch_recompute_generic(uint8_t* rx, size_t L, int t, cudaStream_t 
   cudaError_t err = set_smem((const void*)k_recompute_generic, smem);
   if (err != cudaSuccess) return err;
   k_recompute_generic<<<(unsigned)slices(L), kThreads, smem, s>>>(rx, L, t);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -130,7 +182,32 @@ cudaError_t launch_scale(const uint8_t* src, uint8_t* dst, size_t len, uint8_t c
   if (blocks > 148 * 16) blocks = 148 * 16;
   if (blocks == 0) return cudaSuccess;
   k_scale<<<(unsigned)blocks, 256, 0, s>>>(src, dst, len, c);
+  count_launches(1);
   return cudaGetLastError();
 }
 
+}  // namespace afrs
+
+namespace afrs {
+namespace {
+unsigned stream_grid(size_t work) {
+  size_t blocks = (work + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  return (unsigned)(blocks ? blocks : 1);
+}
+}  // namespace
+
+cudaError_t launch_xor_into(uint8_t* dst, const uint8_t* src, size_t len, cudaStream_t s) {
+  if (len == 0) return cudaSuccess;
+  k_xor_into<<<stream_grid(len / 16 + 1), 256, 0, s>>>(dst, src, len);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_nonzero(const uint8_t* src, size_t len, unsigned long long* count, cudaStream_t s) {
+  if (len == 0) return cudaSuccess;
+  k_count_nonzero<<<stream_grid(len / 16 + 1), 256, 0, s>>>(src, len, count);
+  count_launches(1);
+  return cudaGetLastError();
+}
 }  // namespace afrs

@@ -8,16 +8,19 @@
 //
 // Transforms of 2^k rows, k >= 5, run as three phase kernels (radix 16 x
 // 2^(k-4)):
-//   bottom pass: levels 0..3 on 16 contiguous rows (group g = row >> 4);
-//   top pass:    levels 4..k-1 on rows {b + 16 m};
-//   bottom pass of the next transform.
+//   bottom pass (b1): levels 0..3 on 16 contiguous rows (group g = row >> 4);
+//   top pass (p2):    levels 4..k-1 on rows {b + 16 m};
+//   bottom pass (b3) of the next transform.
 // The code of a bottom pass depends on g (its twiddles do), so each CTA runs
 // one g (blockIdx.y) over many columns: every fetched instruction is used by
-// all warps of the CTA.  (A single kernel holding all rows of a column tile
-// in shared memory runs each variant once per tile and is bound by
-// instruction fetch: ~800 KB of straight-line code for n = 256.)
-// Between phases the rows stay bit-sliced in a scratch buffer sized to stay
-// resident in L2; long shards are processed in column batches.
+// all warps of the CTA.  A bottom group is shared by a warp pair, 8 rows per
+// warp: levels 0..2 stay inside a warp and level 3 goes through shared
+// memory, which halves the registers per thread and the code per variant.
+// (A single kernel holding all rows of a column tile in shared memory runs
+// each variant once per tile and is bound by instruction fetch: ~800 KB of
+// straight-line code for n = 256.)
+// Between phases the rows stay bit-sliced in a scratch buffer (128 MiB at
+// most, largely L2-resident); long shards are processed in column batches.
 // Transforms with k <= 4 run entirely inside one thread.
 #pragma once
 #include "afrs_internal.h"
@@ -824,6 +827,7 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
     }
     const size_t slices = (a.L + 1023) / 1024;
     fn<<<(unsigned)((slices + 7) / 8), kThreads, smem, s>>>(a);
+    count_launches(1);
     return cudaGetLastError();
   } else {
     constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
@@ -837,6 +841,7 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
       k_enc_b1<LOGN, LOGT><<<dim3(gs, C * G), kSplitThreads, kStage8Bytes, s>>>(a, bt);
       k_enc_p2<LOGN, LOGT><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
       k_enc_b3<LOGN, LOGT><<<dim3(gs, G), kSplitThreads, kStage8Bytes, s>>>(a, bt);
+      count_launches(3);
     }
     return cudaGetLastError();
   }
@@ -847,6 +852,7 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
   if constexpr (LOGN <= 4) {
     const size_t slices = (a.L + 1023) / 1024;
     k_rec_small<LOGN><<<(unsigned)((slices + 7) / 8), kThreads, 0, s>>>(a);
+    count_launches(1);
     return cudaGetLastError();
   } else {
     constexpr int N = 1 << LOGN, G = N / 16;
@@ -869,6 +875,7 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
       k_rec_b1<LOGN><<<dim3(gs, G), kSplitThreads, kStage8Bytes, s>>>(a, bt, loc);
       k_rec_p2<LOGN><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
       k_rec_b3<LOGN><<<dim3(gs, gl.count), kSplitThreads, kStage8Bytes, s>>>(a, bt, gl, loc);
+      count_launches(3);
     }
     return cudaGetLastError();
   }

@@ -230,10 +230,12 @@ def main():
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
+    launches0 = afrs.lib().afrs_kernel_launches()
     start.record(stream)
     for i in range(args.steps):
         step(args.warmup + i, evs[i])
     end.record(stream)
+    launches = afrs.lib().afrs_kernel_launches() - launches0
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -302,7 +304,7 @@ def main():
         "clocks": clk,
         "e2e": {"value": round(e2e_value, 3), "unit": "GB/s",
                 "h2d_bytes_per_step": k * L + n * L, "d2h_bytes_per_step": t * L + t * L},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": int(launches),
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -81,6 +81,16 @@ int afrs_recover_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* d_received,
 int afrs_recompute_data_from_parity_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* d_received,
                                         size_t shard_len, void* stream);
 
+/* Sharded form of Codec::compute_syndrome_scalar (rs/src/codec.rs:269-301):
+ * d_syndrome (t shards of shard_len bytes, not overlapping d_received) =
+ * XOR over chunks i < n/t of IFFT_t(shards it..(i+1)t-1 of d_received,
+ * omega_{it}); all zero iff d_received (n shards, parity first) is a
+ * codeword.  If d_nonzero is not NULL, *d_nonzero (device memory) is set to
+ * the number of nonzero syndrome bytes (0 for a codeword).  The reference has
+ * only the scalar form (one column). */
+int afrs_syndrome_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, const uint8_t* d_received, size_t shard_len,
+                      uint8_t* d_syndrome, unsigned long long* d_nonzero, void* stream);
+
 /* The Kernel trait (rs/src/kernel/mod.rs:7-24) on device buffers:
  * fft_sharded / ifft_sharded over 2^k shards at coset beta, in place, and
  * scale (dst = scalar * src, dst may equal src). */
@@ -139,6 +149,11 @@ int afrs_recover_dev_noalloc(uint32_t n, uint32_t t, uint8_t* d_received, size_t
 
 /* Library build information (kernel set, arch) for logs. */
 const char* afrs_version(void);
+
+/* Number of CUDA kernels this library has launched in this process, over
+ * every context and entry point (a diagnostic for benchmarks and tests; no
+ * counterpart in the reference). */
+uint64_t afrs_kernel_launches(void);
 
 #ifdef __cplusplus
 }

@@ -154,6 +154,20 @@ def recover_leopard_form(n: int, t: int, received: np.ndarray, shard_len: int, p
     return bool(r)
 
 
+def syndrome_sharded(n: int, t: int, received: np.ndarray, shard_len: int) -> np.ndarray:
+    """Sharded form of Codec::compute_syndrome_scalar (codec.rs:269-301):
+    s = XOR over chunks i < n/t of IFFT_t(received rows it..(i+1)t-1, omega_{it}),
+    t shards of shard_len bytes; all zero iff `received` is a codeword."""
+    k = t.bit_length() - 1
+    omega = tables().subspace
+    syn = np.zeros(t * shard_len, np.uint8)
+    for i in range(n // t):
+        w = np.ascontiguousarray(received[i * t * shard_len:(i + 1) * t * shard_len]).copy()
+        ifft_sharded(w, shard_len, k, int(omega[i * t]))
+        syn ^= w
+    return syn
+
+
 def recompute_data_from_parity_sharded(n: int, t: int, received: np.ndarray, shard_len: int) -> None:
     ws = np.zeros(t * shard_len, np.uint8)
     lib().orc_recompute_data_from_parity_sharded(n, t, _p(received), _p(ws), ctypes.c_size_t(shard_len))

@@ -111,6 +111,18 @@ def encode_column(n: int, t: int, msg: list[int]) -> list[int]:
     return par
 
 
+def syndrome_column(n: int, t: int, received: list[int]) -> list[int]:
+    """rs/src/codec.rs:269-301 (compute_syndrome_scalar): XOR over chunks i of
+    IFFT_t(chunk i, omega_{it}); the t syndrome symbols."""
+    k_log = t.bit_length() - 1
+    syn = [0] * t
+    for i in range(n // t):
+        w = list(received[i * t:(i + 1) * t])
+        ifft(w, k_log, OMEGA[i * t])
+        syn = [s ^ x for s, x in zip(syn, w)]
+    return syn
+
+
 def recover_column(n: int, t: int, received: list[int], positions: list[int]) -> list[int]:
     """rs/src/codec.rs:479-569 for one byte column; returns the new column."""
     e = len(positions)

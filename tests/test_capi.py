@@ -37,6 +37,7 @@ def test_null_context_is_einval(afrs):
     assert b"NULL" in lib.afrs_last_error()
     assert lib.afrs_recover_dev(None, 4, 2, None, 16, None, 1, None) == afrs._lib.AFRS_EINVAL
     assert lib.afrs_version().startswith(b"afrs_b200")
+    assert lib.afrs_kernel_launches() >= 0
 
 
 def test_no_device_context_fails_cleanly(afrs):

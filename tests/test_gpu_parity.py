@@ -259,3 +259,24 @@ def test_batch_equals_per_call_path_and_reports_status(afrs):
                 ref[p * j.shard_len:(p + 1) * j.shard_len] = 0
             afrs.Codec(j.n, j.t).recover_erasure_shards(ref, None, j.shard_len, j.positions)
         assert torch.equal(ref, j.dst)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t", PAIRS_ALL)
+@pytest.mark.parametrize("L", [1, 33, 1029])
+def test_syndrome_matches_oracle(afrs, n, t, L):
+    """Sharded syndrome (codec.rs:269-301): zero on codewords, equal to the
+    oracle's on a word with corrupted bytes in parity and message shards."""
+    msg, par = _codeword(n, t, L, seed=n * 17 + t + L)
+    cw = np.concatenate([par, msg])
+    codec = afrs.Codec(n, t)
+    syn, nz = codec.syndrome_sharded(torch.from_numpy(cw).cuda(), L)
+    assert not syn.cpu().numpy().any() and int(nz.item()) == 0
+    bad = cw.copy()
+    rng = np.random.default_rng(n + t + L)
+    for i in rng.choice(n * L, min(5, n * L), replace=False):
+        bad[i] ^= int(rng.integers(1, 256))
+    ref = oracle.syndrome_sharded(n, t, bad, L)
+    syn, nz = codec.syndrome_sharded(torch.from_numpy(bad).cuda(), L)
+    assert (syn.cpu().numpy() == ref).all()
+    assert int(nz.item()) == int(np.count_nonzero(ref))

@@ -280,3 +280,24 @@ def test_encode_accumulates_into_parity():
     f = p0.copy()
     oracle.fft_sharded(f, L, 3, 0)
     assert (acc == (zero ^ f)).all()
+
+
+@pytest.mark.parametrize("n,t", [(4, 2), (16, 4), (64, 16), (256, 128)])
+def test_syndrome_restatements_agree(n, t):
+    """oracle.syndrome_sharded (numpy over the C transforms) and the
+    pure-Python scalar form (codec.rs:269-301) on every column; zero on a
+    codeword."""
+    from oracle import pyref
+
+    L = 3
+    msg = oracle.random_bytes((n - t) * L, n + t)
+    par = np.zeros(t * L, np.uint8)
+    oracle.encode_systematic_sharded(n, t, msg, par, L)
+    cw = np.concatenate([par, msg])
+    assert not oracle.syndrome_sharded(n, t, cw, L).any()
+    bad = cw.copy()
+    bad[::7] ^= 0x33
+    syn = oracle.syndrome_sharded(n, t, bad, L)
+    for c in range(L):
+        col = [int(bad[r * L + c]) for r in range(n)]
+        assert pyref.syndrome_column(n, t, col) == [int(syn[r * L + c]) for r in range(t)]
