@@ -106,9 +106,11 @@ def _nbytes(x) -> int:
 class Codec:
     """Mirror of ``Rs::<N, T>`` (rs/src/lib.rs:20-45) running on the GPU."""
 
-    def __init__(self, n: int, t: int, device: int = 0):
+    def __init__(self, n: int, t: int, device: int = 0, context: "Context | None" = None):
         self.n, self.t = int(n), int(t)
-        self.ctx = Context.get(device)
+        # A context's scratch serves one operation at a time; codecs that
+        # should run concurrently on different streams take their own.
+        self.ctx = context if context is not None else Context.get(device)
 
     def _sizes(self, shard_len: int, **bufs) -> None:
         want = {"message": (self.n - self.t) * shard_len, "parity": self.t * shard_len,

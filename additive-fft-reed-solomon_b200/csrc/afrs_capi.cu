@@ -28,6 +28,9 @@ struct afrs_ctx {
   size_t batch_host_bytes[2];
   cudaEvent_t batch_free[2];  // recorded after each batch of the slot
   int batch_slot;
+  // Staged host-buffer path: copy streams and per-slot events.
+  cudaStream_t copy_in, copy_out;
+  cudaEvent_t ev_in[2], ev_cmp[2], ev_out[2];
   std::recursive_mutex mu;
 };
 
@@ -97,9 +100,23 @@ constexpr size_t kWorkCap = (size_t)128 << 20;
 // Grows the context's phase scratch to min(need, kWorkCap) and orders this
 // call after the previous user of the scratch (calls on different streams
 // would otherwise share it concurrently).
+bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone;
+}
+
+// Inside a stream capture (CUDA graphs) the scratch must already be large
+// enough (one call of the same shape before capturing grows it), and the
+// ordering of the context's users is the caller's: the capture records no
+// dependency on work outside the graph.
 cudaError_t acquire_work(afrs_ctx* c, size_t need, cudaStream_t s, afrs::ScratchArena* out) {
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   if (need > kWorkCap) need = kWorkCap;
+  if (capturing(s)) {
+    if (need > c->work_bytes) return cudaErrorStreamCaptureUnsupported;
+    *out = afrs::ScratchArena{c->work, c->work_bytes};
+    return cudaSuccess;
+  }
   if (need > c->work_bytes) {
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return e;
@@ -116,7 +133,9 @@ cudaError_t acquire_work(afrs_ctx* c, size_t need, cudaStream_t s, afrs::Scratch
   return cudaSuccess;
 }
 
-cudaError_t release_work(afrs_ctx* c, cudaStream_t s) { return cudaEventRecord(c->work_free, s); }
+cudaError_t release_work(afrs_ctx* c, cudaStream_t s) {
+  return capturing(s) ? cudaSuccess : cudaEventRecord(c->work_free, s);
+}
 
 int launch_encode(afrs_ctx* c, const afrs::EncodeArgs& a, cudaStream_t s) {
   afrs::ScratchArena sc{nullptr, 0};
@@ -140,6 +159,118 @@ int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
   return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "recover launch");
 }
 
+
+// ---- staged host-buffer path (afrs_encode, afrs_recover) -------------------
+// The shard columns are cut into windows of W columns.  Window i uses staging
+// slot i % 2 (a compact n x w block of device memory) and three streams:
+// copy_in (host -> slot, only the rows the operation reads), the context
+// stream (kernels, with shard_len = w) and copy_out (slot -> host, only the
+// rows it writes).  Copy-in of window i+1 overlaps the kernels of window i and
+// the copy-out of window i-1, and the two PCIe directions run at once; with
+// page-locked caller buffers the copies are DMA straight to and from them.
+// Rows move as runs of adjacent rows, one 2D copy per run (host pitch L,
+// device pitch w); runs closer than kMergeBytes are merged and the rows in
+// between are copied too, which is harmless: the decoder does not read
+// erased rows, and survivor rows copied back hold the bytes they came with.
+std::atomic<uint64_t> g_h2d_bytes{0}, g_d2h_bytes{0};
+
+constexpr int kSlots = 2;
+constexpr size_t kWindowBytes = (size_t)4 << 20;  // n * W per window
+constexpr size_t kMergeBytes = (size_t)128 << 10;
+
+size_t window_cols(uint32_t n, size_t L) {
+  size_t W = kWindowBytes / n / 1024 * 1024;
+  if (W < 1024) W = 1024;
+  return W >= L ? L : W;
+}
+
+struct RowRun {
+  uint32_t r0, rows;
+};
+
+// Runs of rows with sel[r] set, gaps of at most kMergeBytes / w rows merged.
+std::vector<RowRun> row_runs(const bool* sel, uint32_t n, size_t w) {
+  std::vector<RowRun> runs;
+  const size_t max_gap = w ? kMergeBytes / w : 0;
+  for (uint32_t r = 0; r < n; r++) {
+    if (!sel[r]) continue;
+    if (!runs.empty()) {
+      RowRun& b = runs.back();
+      const uint32_t end = b.r0 + b.rows;
+      if (r - end <= max_gap) {
+        b.rows = r + 1 - b.r0;
+        continue;
+      }
+    }
+    runs.push_back(RowRun{r, 1});
+  }
+  return runs;
+}
+
+cudaError_t copy_rows_h2d(uint8_t* dev, size_t w, const uint8_t* host, size_t L, size_t c0,
+                          const std::vector<RowRun>& runs, cudaStream_t s) {
+  for (const RowRun& q : runs) {
+    cudaError_t e = cudaMemcpy2DAsync(dev + (size_t)q.r0 * w, w, host + (size_t)q.r0 * L + c0, L, w, q.rows,
+                                      cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    g_h2d_bytes.fetch_add((uint64_t)w * q.rows, std::memory_order_relaxed);
+  }
+  return cudaSuccess;
+}
+
+cudaError_t copy_rows_d2h(uint8_t* host, size_t L, size_t c0, const uint8_t* dev, size_t w,
+                          const std::vector<RowRun>& runs, cudaStream_t s) {
+  for (const RowRun& q : runs) {
+    cudaError_t e = cudaMemcpy2DAsync(host + (size_t)q.r0 * L + c0, L, dev + (size_t)q.r0 * w, w, w, q.rows,
+                                      cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    g_d2h_bytes.fetch_add((uint64_t)w * q.rows, std::memory_order_relaxed);
+  }
+  return cudaSuccess;
+}
+
+// Waits for all three streams (also on error paths, so that no copy still
+// references the caller's buffers after the call returns).
+cudaError_t drain(afrs_ctx* c) {
+  cudaError_t a = cudaStreamSynchronize(c->copy_in);
+  cudaError_t b = cudaStreamSynchronize(c->stream);
+  cudaError_t d = cudaStreamSynchronize(c->copy_out);
+  return a != cudaSuccess ? a : (b != cudaSuccess ? b : d);
+}
+
+// Runs `body(slot_base, w, c0)` per window with the copies around it.
+// `in` / `out` describe the host rows (a codeword of `rows` rows) to stage.
+template <class Launch>
+int staged(afrs_ctx* c, uint32_t rows, size_t L, const uint8_t* h_in, const bool* sel_in, uint8_t* h_out,
+           const bool* sel_out, Launch&& launch) {
+  const size_t W = window_cols(rows, L);
+  cudaError_t e = ensure_scratch(c, (size_t)kSlots * rows * W);
+  if (e != cudaSuccess) return cuda_fail(e, "staging allocation");
+  int slot = 0;
+  for (size_t c0 = 0; c0 < L; c0 += W, slot ^= 1) {
+    const size_t w = (L - c0 < W) ? L - c0 : W;
+    uint8_t* base = c->scratch + (size_t)slot * rows * W;
+    const std::vector<RowRun> rin = row_runs(sel_in, rows, w), rout = row_runs(sel_out, rows, w);
+    int r = AFRS_OK;
+    if ((e = cudaStreamWaitEvent(c->copy_in, c->ev_out[slot], 0)) == cudaSuccess &&
+        (e = copy_rows_h2d(base, w, h_in, L, c0, rin, c->copy_in)) == cudaSuccess &&
+        (e = cudaEventRecord(c->ev_in[slot], c->copy_in)) == cudaSuccess &&
+        (e = cudaStreamWaitEvent(c->stream, c->ev_in[slot], 0)) == cudaSuccess) {
+      r = launch(base, w);
+      if (r == AFRS_OK && (e = cudaEventRecord(c->ev_cmp[slot], c->stream)) == cudaSuccess &&
+          (e = cudaStreamWaitEvent(c->copy_out, c->ev_cmp[slot], 0)) == cudaSuccess &&
+          (e = copy_rows_d2h(h_out, L, c0, base, w, rout, c->copy_out)) == cudaSuccess)
+        e = cudaEventRecord(c->ev_out[slot], c->copy_out);
+    }
+    if (r != AFRS_OK || e != cudaSuccess) {
+      drain(c);
+      return r != AFRS_OK ? r : cuda_fail(e, "staged copy");
+    }
+  }
+  if ((e = drain(c)) != cudaSuccess) return cuda_fail(e, "staged operation");
+  return AFRS_OK;
+}
+
 }  // namespace
 
 namespace afrs {
@@ -153,6 +284,11 @@ extern "C" {
 const char* afrs_last_error(void) { return g_err; }
 
 uint64_t afrs_kernel_launches(void) { return afrs::g_launches.load(std::memory_order_relaxed); }
+
+void afrs_staged_bytes(uint64_t* h2d, uint64_t* d2h) {
+  if (h2d) *h2d = g_h2d_bytes.load(std::memory_order_relaxed);
+  if (d2h) *d2h = g_d2h_bytes.load(std::memory_order_relaxed);
+}
 
 const char* afrs_version(void) { return "afrs_b200 0.1 sm_100a (bit-sliced GF(2^8) additive FFT)"; }
 
@@ -186,6 +322,13 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
   e = cudaEventCreateWithFlags(&c->work_free, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->batch_free[0], cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->batch_free[1], cudaEventDisableTiming);
+  for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+    e = cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_cmp[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_out[i], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     cudaStreamDestroy(c->stream);
     delete c;
@@ -207,6 +350,13 @@ void afrs_ctx_destroy(afrs_ctx* c) {
     cudaEventDestroy(c->batch_free[i]);
   }
   cudaEventDestroy(c->work_free);
+  for (int i = 0; i < 2; i++) {
+    cudaEventDestroy(c->ev_in[i]);
+    cudaEventDestroy(c->ev_cmp[i]);
+    cudaEventDestroy(c->ev_out[i]);
+  }
+  cudaStreamDestroy(c->copy_in);
+  cudaStreamDestroy(c->copy_out);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -255,20 +405,41 @@ int afrs_encode(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* message, uin
   if (!message || !parity) return fail(AFRS_EINVAL, "NULL buffer");
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   DeviceGuard g(c->device);
-  const size_t mb = (size_t)(n - t) * L, pb = (size_t)t * L;
-  cudaError_t e = ensure_scratch(c, mb + pb);
-  if (e != cudaSuccess) return cuda_fail(e, "scratch allocation");
-  uint8_t* dm = c->scratch;
-  uint8_t* dp = c->scratch + mb;
-  if ((e = cudaMemcpyAsync(dm, message, mb, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-    return cuda_fail(e, "H2D message");
-  if (accumulate && (e = cudaMemcpyAsync(dp, parity, pb, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-    return cuda_fail(e, "H2D parity");
-  afrs::EncodeArgs a{dm, dp, L, (int)n, (int)t, accumulate ? 1 : 0};
-  if ((r = launch_encode(c, a, c->stream))) return r;
-  if ((e = cudaMemcpyAsync(parity, dp, pb, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
-    return cuda_fail(e, "D2H parity");
-  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "encode");
+  const uint32_t k = n - t;
+  // Staged as one n-row block per window: message rows 0..k-1, parity rows
+  // k..n-1.  The message and parity host buffers are separate, so each is
+  // its own 2D copy.
+  bool sel_msg[256] = {}, sel_par[256] = {};
+  for (uint32_t r0 = 0; r0 < k; r0++) sel_msg[r0] = true;
+  for (uint32_t r0 = 0; r0 < t; r0++) sel_par[r0] = true;
+  const size_t W = window_cols(n, L);
+  cudaError_t e = ensure_scratch(c, (size_t)kSlots * n * W);
+  if (e != cudaSuccess) return cuda_fail(e, "staging allocation");
+  int slot = 0;
+  for (size_t c0 = 0; c0 < L; c0 += W, slot ^= 1) {
+    const size_t w = (L - c0 < W) ? L - c0 : W;
+    uint8_t* dm = c->scratch + (size_t)slot * n * W;
+    uint8_t* dp = dm + (size_t)k * w;
+    const std::vector<RowRun> rm = row_runs(sel_msg, k, w), rp = row_runs(sel_par, t, w);
+    r = AFRS_OK;
+    if ((e = cudaStreamWaitEvent(c->copy_in, c->ev_out[slot], 0)) == cudaSuccess &&
+        (e = copy_rows_h2d(dm, w, message, L, c0, rm, c->copy_in)) == cudaSuccess &&
+        (!accumulate || (e = copy_rows_h2d(dp, w, parity, L, c0, rp, c->copy_in)) == cudaSuccess) &&
+        (e = cudaEventRecord(c->ev_in[slot], c->copy_in)) == cudaSuccess &&
+        (e = cudaStreamWaitEvent(c->stream, c->ev_in[slot], 0)) == cudaSuccess) {
+      afrs::EncodeArgs a{dm, dp, w, (int)n, (int)t, accumulate ? 1 : 0};
+      r = launch_encode(c, a, c->stream);
+      if (r == AFRS_OK && (e = cudaEventRecord(c->ev_cmp[slot], c->stream)) == cudaSuccess &&
+          (e = cudaStreamWaitEvent(c->copy_out, c->ev_cmp[slot], 0)) == cudaSuccess &&
+          (e = copy_rows_d2h(parity, L, c0, dp, w, rp, c->copy_out)) == cudaSuccess)
+        e = cudaEventRecord(c->ev_out[slot], c->copy_out);
+    }
+    if (r != AFRS_OK || e != cudaSuccess) {
+      drain(c);
+      return r != AFRS_OK ? r : cuda_fail(e, "encode staging");
+    }
+  }
+  if ((e = drain(c)) != cudaSuccess) return cuda_fail(e, "encode");
   return AFRS_OK;
 }
 
@@ -285,27 +456,22 @@ int afrs_recover(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* received, size_t 
   if (!received) return fail(AFRS_EINVAL, "NULL buffer");
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   DeviceGuard g(c->device);
-  const size_t bytes = (size_t)n * L;
-  cudaError_t e = ensure_scratch(c, bytes);
-  if (e != cudaSuccess) return cuda_fail(e, "scratch allocation");
-  if ((e = cudaMemcpyAsync(c->scratch, received, bytes, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-    return cuda_fail(e, "H2D received");
+  // In: the surviving shards (the decoder reads no erased row).  Out: the
+  // erased shards, the only ones that change.
+  bool erased[256] = {}, survivor[256] = {};
+  for (size_t j = 0; j < e_count; j++) erased[positions[j]] = true;
+  for (uint32_t r0 = 0; r0 < n; r0++) survivor[r0] = !erased[r0];
   afrs::RecoverArgs a{};
-  a.rx = c->scratch;
-  a.L = L;
   a.n = (int)n;
   a.t = (int)t;
   a.e = (int)e_count;
   std::memcpy(a.pos, positions, e_count);
-  if ((r = launch_recover(c, a, c->stream))) return r;
-  // Only the erased shards change: copy just those back.
-  for (size_t j = 0; j < e_count; j++) {
-    const size_t off = (size_t)positions[j] * L;
-    if ((e = cudaMemcpyAsync(received + off, c->scratch + off, L, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
-      return cuda_fail(e, "D2H recovered shard");
-  }
-  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_fail(e, "recover");
-  return 1;
+  r = staged(c, n, L, received, survivor, received, erased, [&](uint8_t* base, size_t w) {
+    a.rx = base;
+    a.L = w;
+    return launch_recover(c, a, c->stream);
+  });
+  return r == AFRS_OK ? 1 : r;
 }
 
 int afrs_recompute_data_from_parity_dev(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* d_received, size_t L,

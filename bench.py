@@ -18,6 +18,7 @@ as their C restatement in oracle/gfni_baseline.c, on all host cores.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import json
 import os
 import statistics
@@ -150,6 +151,8 @@ def main():
     ap.add_argument("--impl", default="afrs", choices=["afrs", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serial", action="store_true", help="encode and recover of a step on one stream")
+    ap.add_argument("--no-graphs", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
     ap.add_argument("--workload", default="codeword", choices=["codeword", "small", "batched", "serving", "large"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -199,29 +202,71 @@ def main():
             rx[p * L:(p + 1) * L] = 0
         rec_bufs.append(torch.from_numpy(rx).to(dev))
         patterns.append(pos)
-    codec = afrs.Codec(n, t, device=local)
+    # One context per operation so that, with overlap, the encode of one
+    # codeword and the recover of another run concurrently on two streams
+    # (a context's scratch serves one operation at a time).
+    codec_e = afrs.Codec(n, t, device=local, context=afrs.Context(local))
+    codec_r = afrs.Codec(n, t, device=local, context=afrs.Context(local))
     stream = torch.cuda.current_stream(dev)
+    overlap = not args.serial
+    s_enc = torch.cuda.Stream(dev) if overlap else stream
+    s_rec = torch.cuda.Stream(dev) if overlap else stream
 
-    def step(i, ev=None):
-        m, p = enc_bufs[i % R]
-        if ev is not None:
-            ev[0].record(stream)
-        codec.encode_parity(m, p, L)
-        if ev is not None:
-            ev[1].record(stream)
-        ok = codec.recover_erasure_shards(rec_bufs[i % R], None, L, patterns[i % R])
-        if ev is not None:
-            ev[2].record(stream)
-        return ok
+    def enc_call(r):
+        m, p = enc_bufs[r]
+        codec_e.encode_parity(m, p, L)
+
+    def rec_call(r):
+        codec_r.recover_erasure_shards(rec_bufs[r], None, L, patterns[r])
 
     for i in range(args.warmup):
-        step(i)
+        with torch.cuda.stream(s_enc):
+            enc_call(i % R)
+        with torch.cuda.stream(s_rec):
+            rec_call(i % R)
     torch.cuda.synchronize()
     # correctness of the measured path on codeword 0
     assert (enc_bufs[0][1].cpu().numpy() == par0).all(), "encode mismatch vs oracle"
     assert (rec_bufs[0].cpu().numpy() == cw0).all(), "recover mismatch vs oracle"
 
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    # CUDA graphs: each operation on each of the R codewords is captured once
+    # (the erasure locator of its pattern is computed on the host at capture)
+    # and replayed, so the timed steps carry no host launch overhead.
+    use_graphs = not args.no_graphs
+    launches_per_step = None
+    if use_graphs:
+        cap = torch.cuda.Stream(dev)
+        g_enc, g_rec = [], []
+        l0 = afrs.lib().afrs_kernel_launches()
+        for r in range(R):
+            ge, gr = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+            with torch.cuda.graph(ge, stream=cap):
+                enc_call(r)
+            with torch.cuda.graph(gr, stream=cap):
+                rec_call(r)
+            g_enc.append(ge)
+            g_rec.append(gr)
+        launches_per_step = (afrs.lib().afrs_kernel_launches() - l0) / R
+
+    def step(i, ev=None):
+        with torch.cuda.stream(s_enc):
+            if ev is not None:
+                ev[0].record(s_enc)
+            g_enc[i % R].replay() if use_graphs else enc_call(i % R)
+            if ev is not None:
+                ev[1].record(s_enc)
+        with torch.cuda.stream(s_rec):
+            if ev is not None:
+                ev[2].record(s_rec)
+            g_rec[i % R].replay() if use_graphs else rec_call(i % R)
+            if ev is not None:
+                ev[3].record(s_rec)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
@@ -232,17 +277,25 @@ def main():
     end = torch.cuda.Event(enable_timing=True)
     launches0 = afrs.lib().afrs_kernel_launches()
     start.record(stream)
+    s_enc.wait_stream(stream)
+    s_rec.wait_stream(stream)
     for i in range(args.steps):
         step(args.warmup + i, evs[i])
+    stream.wait_stream(s_enc)
+    stream.wait_stream(s_rec)
     end.record(stream)
     launches = afrs.lib().afrs_kernel_launches() - launches0
+    if use_graphs:
+        launches = int(round(launches_per_step * args.steps))  # kernel nodes replayed
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
+    assert (enc_bufs[0][1].cpu().numpy() == par0).all(), "encode mismatch after the timed steps"
+    assert (rec_bufs[0].cpu().numpy() == cw0).all(), "recover mismatch after the timed steps"
     elapsed_ms = start.elapsed_time(end)
     enc_ms = [e[0].elapsed_time(e[1]) for e in evs]
-    rec_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    rec_ms = [e[2].elapsed_time(e[3]) for e in evs]
     if world > 1:
         tt = torch.tensor([elapsed_ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -267,19 +320,50 @@ def main():
     for p in pos0:
         h_rx_src[p * L:(p + 1) * L] = 0
     e2e_steps = max(3, min(args.steps, 20))
+
+    def e2e_encode():
+        codec_e.encode_parity(h_msg, h_par, L)
+
+    def e2e_recover():
+        codec_r.recover_erasure_shards(h_rx, None, L, pos0)
+
+    # With overlap, the two operations of a step are issued from two host
+    # threads (the C calls release the GIL), each through its own context.
+    pool = concurrent.futures.ThreadPoolExecutor(2) if overlap else None
+
+    def e2e_step():
+        if pool is None:
+            e2e_encode()
+            e2e_recover()
+        else:
+            fe, fr = pool.submit(e2e_encode), pool.submit(e2e_recover)
+            fe.result()
+            fr.result()
+
     for _ in range(2):
-        codec.encode_parity(h_msg, h_par, L)
         h_rx[:] = h_rx_src
-        codec.recover_erasure_shards(h_rx, None, L, pos0)
+        e2e_step()
     assert (h_par == par0).all() and (h_rx == cw0).all(), "host-API result mismatch"
+
+    def staged():
+        import ctypes
+
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        afrs.lib().afrs_staged_bytes(ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
     e2e_time = 0.0
+    s0 = staged()
     for _ in range(e2e_steps):
         h_rx[:] = h_rx_src  # host-side reset of the erased shards, not timed
         t0 = time.perf_counter()
-        codec.encode_parity(h_msg, h_par, L)
-        codec.recover_erasure_shards(h_rx, None, L, pos0)
+        e2e_step()
         e2e_time += time.perf_counter() - t0
+    s1 = staged()
+    if pool is not None:
+        pool.shutdown()
     e2e_value = world * 2 * op_bytes * e2e_steps / e2e_time / 1e9
+    h2d_step, d2h_step = (s1[0] - s0[0]) // e2e_steps, (s1[1] - s0[1]) // e2e_steps
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -294,6 +378,9 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": n, "k": k, "t": t, "shard_len": L, "erasures": t,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "overlap": "encode and recover of a step on two streams (own contexts)" if overlap
+                   else "encode then recover on one stream",
+                   "launch": "CUDA graph per operation and codeword, replayed" if use_graphs else "eager",
                    "l2": f"inputs rotate over {R} encode + {R} recover codewords (512 MiB > 126 MB L2)"},
         "encode_gbs": round(op_bytes / (enc_avg * 1e-3) / 1e9, 2),
         "recover_gbs": round(op_bytes / (rec_avg * 1e-3) / 1e9, 2),
@@ -303,7 +390,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clk,
         "e2e": {"value": round(e2e_value, 3), "unit": "GB/s",
-                "h2d_bytes_per_step": k * L + n * L, "d2h_bytes_per_step": t * L + t * L},
+                "h2d_bytes_per_step": int(h2d_step), "d2h_bytes_per_step": int(d2h_step)},
         "gpu_launches": int(launches),
     }
     if rank == 0:

@@ -155,6 +155,11 @@ const char* afrs_version(void);
  * counterpart in the reference). */
 uint64_t afrs_kernel_launches(void);
 
+/* Bytes the host-buffer entry points (afrs_encode, afrs_recover) have copied
+ * host -> device and device -> host in this process (a diagnostic; no
+ * counterpart in the reference). */
+void afrs_staged_bytes(uint64_t* h2d, uint64_t* d2h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -280,3 +280,75 @@ def test_syndrome_matches_oracle(afrs, n, t, L):
     syn, nz = codec.syndrome_sharded(torch.from_numpy(bad).cuda(), L)
     assert (syn.cpu().numpy() == ref).all()
     assert int(nz.item()) == int(np.count_nonzero(ref))
+
+
+def _pinned(a):
+    return torch.from_numpy(a).pin_memory().numpy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t,L", [(256, 128, 3 * 16384 + 1000), (64, 16, 2 * 65536 + 77), (16, 8, 300000),
+                                   (256, 32, 16384)])
+@pytest.mark.parametrize("pinned", [True, False])
+def test_staged_host_path_windows_and_runs(afrs, n, t, L, pinned):
+    """The host-buffer entry points stage column windows (4 MiB per window:
+    16 KiB columns at n = 256) through two device slots and copy only the
+    rows an operation reads or writes, as merged runs.  Shards spanning
+    several windows with a ragged last one, page-locked and pageable buffers,
+    accumulate, and erasure patterns with long runs, isolated rows and gaps."""
+    msg, par = _codeword(n, t, L, seed=n + L)
+    cw = np.concatenate([par, msg])
+    codec = afrs.Codec(n, t)
+    h_msg = _pinned(msg) if pinned else msg.copy()
+    got = _pinned(np.zeros(t * L, np.uint8)) if pinned else np.zeros(t * L, np.uint8)
+    codec.encode_systematic_sharded(h_msg, got, None, L)
+    assert (got == par).all()
+    p0 = oracle.random_bytes(t * L, 9)
+    ref = p0.copy()
+    oracle.encode_systematic_sharded(n, t, msg, ref, L)
+    acc = _pinned(p0) if pinned else p0.copy()
+    codec.encode_systematic_sharded(h_msg, acc, None, L)
+    assert (acc == ref).all()
+    rng = np.random.default_rng(n * 3 + t)
+    patterns = [sorted(rng.choice(n, t, replace=False).tolist()), list(range(n - t, n)), list(range(0, n, n // t))[:t],
+                [0, n - 1], [n // 2]]
+    for pos in patterns:
+        rx = _erase(cw, L, pos)
+        if pinned:
+            rx = _pinned(rx)
+        assert codec.recover_erasure_shards(rx, None, L, pos)
+        assert (rx == cw).all(), pos
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t,L", [(256, 128, 65536), (64, 32, 1024), (16, 8, 5000)])
+def test_cuda_graph_capture_and_replay(afrs, n, t, L):
+    """Device entry points inside stream capture: one eager call grows the
+    scratch, then encode and recover are captured into CUDA graphs and
+    replayed; results equal the oracle's."""
+    msg, par = _codeword(n, t, L, seed=n + 7 * t)
+    cw = np.concatenate([par, msg])
+    pos = sorted(np.random.default_rng(n).choice(n, t, replace=False).tolist())
+    codec = afrs.Codec(n, t, context=afrs.Context(0))
+    d_msg = torch.from_numpy(msg).cuda()
+    d_par = torch.zeros(t * L, dtype=torch.uint8, device="cuda")
+    d_rx = torch.from_numpy(_erase(cw, L, pos)).cuda()
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        codec.encode_parity(d_msg, d_par, L)
+        assert codec.recover_erasure_shards(d_rx.clone(), None, L, pos)
+    torch.cuda.synchronize()
+    d_par.zero_()
+    ge, gr = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(ge, stream=side):
+        codec.encode_parity(d_msg, d_par, L)
+    with torch.cuda.graph(gr, stream=side):
+        codec.recover_erasure_shards(d_rx, None, L, pos)
+    torch.cuda.synchronize()
+    assert not d_par.any()  # capture does not run the kernels
+    for _ in range(3):
+        ge.replay()
+        gr.replay()
+    torch.cuda.synchronize()
+    assert (d_par.cpu().numpy() == par).all()
+    assert (d_rx.cpu().numpy() == cw).all()
