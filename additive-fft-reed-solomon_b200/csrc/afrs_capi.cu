@@ -1,4 +1,5 @@
 // C ABI of libafrs_b200.so (declared in include/afrs.h).
+#include <cuda.h>  // driver types for cuPointerGetAttribute (resolved at run time, not linked)
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -31,6 +32,8 @@ struct afrs_ctx {
   // Staged host-buffer path: copy streams and per-slot events.
   cudaStream_t copy_in, copy_out;
   cudaEvent_t ev_in[2], ev_cmp[2], ev_out[2];
+  size_t window_bytes, merge_bytes;  // staging parameters (afrs_ctx_set_staging)
+  int direct_mode;                   // AFRS_HOST_* (afrs_ctx_set_staging)
   std::recursive_mutex mu;
 };
 
@@ -160,6 +163,102 @@ int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
 }
 
 
+// Waits for all three streams (also on error paths, so that no copy still
+// references the caller's buffers after the call returns).
+cudaError_t drain(afrs_ctx* c) {
+  cudaError_t a = cudaStreamSynchronize(c->copy_in);
+  cudaError_t b = cudaStreamSynchronize(c->stream);
+  cudaError_t d = cudaStreamSynchronize(c->copy_out);
+  return a != cudaSuccess ? a : (b != cudaSuccess ? b : d);
+}
+
+// ---- direct path for page-locked host buffers -------------------------------
+// Page-locked host memory that is mapped into the device's address space can
+// be read and written by the kernels themselves over PCIe: the decoder then
+// reads exactly the surviving shards and writes exactly the erased ones (the
+// encoder: message in, parity out), with no staging copies at all.  A range
+// qualifies only if it lies inside one such allocation (checked with the
+// driver's allocation-range attributes); anything else takes the staged path.
+using PtrAttrFn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+
+PtrAttrFn ptr_attr_fn() {
+  static PtrAttrFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<PtrAttrFn>(f);
+  }();
+  return fn;
+}
+
+// Device address of host range [p, p + bytes) when the kernels may access it
+// directly, nullptr otherwise.
+uint8_t* mapped_host_range(const void* p, size_t bytes) {
+  PtrAttrFn fn = ptr_attr_fn();
+  if (!fn || !p || !bytes) return nullptr;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  const CUdeviceptr hp = (CUdeviceptr)(uintptr_t)p;
+  if (fn(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, hp) != CUDA_SUCCESS ||
+      fn(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, hp) != CUDA_SUCCESS)
+    return nullptr;
+  if (hp < start || hp - start > size || bytes > size - (hp - start)) return nullptr;
+  return static_cast<uint8_t*>(a.devicePointer);
+}
+
+// Runs `launch(args, arena, stream)` over column windows of the whole shard
+// width: up to kDirectWindows windows of the same rows (pitch = full shard
+// length) alternate between two streams, each with half of the scratch, so
+// that one window's reads of host memory overlap another's writes.
+constexpr int kDirectWindows = 4;
+
+template <class Args, class Need, class Shift, class Launch>
+int run_direct(afrs_ctx* c, const Args& a, Need need_for, Shift shift, Launch launch, const char* what) {
+  const size_t L = a.L;
+  size_t W = L;
+  if (L >= 4096) W = ((L + kDirectWindows - 1) / kDirectWindows + 1023) / 1024 * 1024;
+  const size_t need1 = need_for(W);
+  cudaStream_t s0 = c->stream, s1 = c->copy_in;
+  afrs::ScratchArena sc{nullptr, 0};
+  cudaError_t e = cudaSuccess;
+  if (need1 && (e = acquire_work(c, 2 * need1, s0, &sc)) != cudaSuccess) return cuda_fail(e, what);
+  const size_t half = (sc.bytes / 2) & ~(size_t)255;
+  const bool two = W < L && (!need1 || half >= need1);
+  if (two && ((e = cudaEventRecord(c->ev_in[0], s0)) != cudaSuccess ||
+              (e = cudaStreamWaitEvent(s1, c->ev_in[0], 0)) != cudaSuccess))
+    return cuda_fail(e, what);
+  int idx = 0;
+  for (size_t c0 = 0; c0 < L && e == cudaSuccess; c0 += W, idx++) {
+    const int k = two ? (idx & 1) : 0;
+    Args w = a;
+    shift(w, c0);
+    w.L = (L - c0 < W) ? L - c0 : W;
+    w.pitch = L;
+    afrs::ScratchArena sub{nullptr, 0};
+    if (need1) {
+      sub.ptr = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(sc.ptr) + (size_t)k * half);
+      sub.bytes = two ? half : sc.bytes;
+    }
+    e = launch(w, sub, k ? s1 : s0);
+  }
+  cudaError_t e2 = cudaSuccess;
+  if (two && (e2 = cudaEventRecord(c->ev_in[1], s1)) == cudaSuccess) e2 = cudaStreamWaitEvent(s0, c->ev_in[1], 0);
+  if (need1 && e2 == cudaSuccess) e2 = release_work(c, s0);
+  cudaError_t e3 = drain(c);
+  if (e == cudaSuccess) e = e2 != cudaSuccess ? e2 : e3;
+  return e == cudaSuccess ? AFRS_OK : cuda_fail(e, what);
+}
+
 // ---- staged host-buffer path (afrs_encode, afrs_recover) -------------------
 // The shard columns are cut into windows of W columns.  Window i uses staging
 // slot i % 2 (a compact n x w block of device memory) and three streams:
@@ -175,11 +274,11 @@ int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
 std::atomic<uint64_t> g_h2d_bytes{0}, g_d2h_bytes{0};
 
 constexpr int kSlots = 2;
-constexpr size_t kWindowBytes = (size_t)4 << 20;  // n * W per window
-constexpr size_t kMergeBytes = (size_t)128 << 10;
+constexpr size_t kWindowBytes = (size_t)4 << 20;  // default n * W per window
+constexpr size_t kMergeBytes = (size_t)128 << 10;  // default gap merged into a run
 
-size_t window_cols(uint32_t n, size_t L) {
-  size_t W = kWindowBytes / n / 1024 * 1024;
+size_t window_cols(const afrs_ctx* c, uint32_t n, size_t L) {
+  size_t W = c->window_bytes / n / 1024 * 1024;
   if (W < 1024) W = 1024;
   return W >= L ? L : W;
 }
@@ -188,10 +287,10 @@ struct RowRun {
   uint32_t r0, rows;
 };
 
-// Runs of rows with sel[r] set, gaps of at most kMergeBytes / w rows merged.
-std::vector<RowRun> row_runs(const bool* sel, uint32_t n, size_t w) {
+// Runs of rows with sel[r] set, gaps of at most merge_bytes / w rows merged.
+std::vector<RowRun> row_runs(const bool* sel, uint32_t n, size_t w, size_t merge_bytes) {
   std::vector<RowRun> runs;
-  const size_t max_gap = w ? kMergeBytes / w : 0;
+  const size_t max_gap = w ? merge_bytes / w : 0;
   for (uint32_t r = 0; r < n; r++) {
     if (!sel[r]) continue;
     if (!runs.empty()) {
@@ -229,28 +328,21 @@ cudaError_t copy_rows_d2h(uint8_t* host, size_t L, size_t c0, const uint8_t* dev
   return cudaSuccess;
 }
 
-// Waits for all three streams (also on error paths, so that no copy still
-// references the caller's buffers after the call returns).
-cudaError_t drain(afrs_ctx* c) {
-  cudaError_t a = cudaStreamSynchronize(c->copy_in);
-  cudaError_t b = cudaStreamSynchronize(c->stream);
-  cudaError_t d = cudaStreamSynchronize(c->copy_out);
-  return a != cudaSuccess ? a : (b != cudaSuccess ? b : d);
-}
 
 // Runs `body(slot_base, w, c0)` per window with the copies around it.
 // `in` / `out` describe the host rows (a codeword of `rows` rows) to stage.
 template <class Launch>
 int staged(afrs_ctx* c, uint32_t rows, size_t L, const uint8_t* h_in, const bool* sel_in, uint8_t* h_out,
            const bool* sel_out, Launch&& launch) {
-  const size_t W = window_cols(rows, L);
+  const size_t W = window_cols(c, rows, L);
   cudaError_t e = ensure_scratch(c, (size_t)kSlots * rows * W);
   if (e != cudaSuccess) return cuda_fail(e, "staging allocation");
   int slot = 0;
   for (size_t c0 = 0; c0 < L; c0 += W, slot ^= 1) {
     const size_t w = (L - c0 < W) ? L - c0 : W;
     uint8_t* base = c->scratch + (size_t)slot * rows * W;
-    const std::vector<RowRun> rin = row_runs(sel_in, rows, w), rout = row_runs(sel_out, rows, w);
+    const std::vector<RowRun> rin = row_runs(sel_in, rows, w, c->merge_bytes),
+                              rout = row_runs(sel_out, rows, w, c->merge_bytes);
     int r = AFRS_OK;
     if ((e = cudaStreamWaitEvent(c->copy_in, c->ev_out[slot], 0)) == cudaSuccess &&
         (e = copy_rows_h2d(base, w, h_in, L, c0, rin, c->copy_in)) == cudaSuccess &&
@@ -283,6 +375,17 @@ extern "C" {
 
 const char* afrs_last_error(void) { return g_err; }
 
+int afrs_ctx_set_staging(afrs_ctx* c, size_t window_bytes, size_t merge_bytes, int host_mode) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (host_mode < AFRS_HOST_AUTO || host_mode > AFRS_HOST_DIRECT)
+    return fail(AFRS_EINVAL, "host_mode %d is not an AFRS_HOST_* value", host_mode);
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->direct_mode = host_mode;
+  c->window_bytes = window_bytes ? window_bytes : kWindowBytes;
+  c->merge_bytes = merge_bytes == (size_t)-1 ? 0 : (merge_bytes ? merge_bytes : kMergeBytes);
+  return AFRS_OK;
+}
+
 uint64_t afrs_kernel_launches(void) { return afrs::g_launches.load(std::memory_order_relaxed); }
 
 void afrs_staged_bytes(uint64_t* h2d, uint64_t* d2h) {
@@ -314,6 +417,9 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
     c->batch_host_bytes[i] = 0;
   }
   c->batch_slot = 0;
+  c->window_bytes = kWindowBytes;
+  c->merge_bytes = kMergeBytes;
+  c->direct_mode = AFRS_HOST_AUTO;
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete c;
@@ -406,13 +512,35 @@ int afrs_encode(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* message, uin
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   DeviceGuard g(c->device);
   const uint32_t k = n - t;
+  {
+    const bool want = c->direct_mode == AFRS_HOST_DIRECT;
+    uint8_t* dm = want ? mapped_host_range(message, (size_t)k * L) : nullptr;
+    uint8_t* dp = dm ? mapped_host_range(parity, (size_t)t * L) : nullptr;
+    if (dm && dp) {
+      afrs::EncodeArgs a{dm, dp, L, (int)n, (int)t, accumulate ? 1 : 0};
+      r = run_direct(
+          c, a, [&](size_t W) { return afrs::scratch_bytes_encode((int)n, (int)t, W); },
+          [](afrs::EncodeArgs& w, size_t c0) {
+            w.msg += c0;
+            w.parity += c0;
+          },
+          [](const afrs::EncodeArgs& w, const afrs::ScratchArena& sc, cudaStream_t s) {
+            return afrs::launch_encode_special(w, sc, s);
+          },
+          "encode (page-locked buffers)");
+      if (r) return r;
+      g_h2d_bytes.fetch_add((uint64_t)(accumulate ? n : k) * L, std::memory_order_relaxed);
+      g_d2h_bytes.fetch_add((uint64_t)t * L, std::memory_order_relaxed);
+      return AFRS_OK;
+    }
+  }
   // Staged as one n-row block per window: message rows 0..k-1, parity rows
   // k..n-1.  The message and parity host buffers are separate, so each is
   // its own 2D copy.
   bool sel_msg[256] = {}, sel_par[256] = {};
   for (uint32_t r0 = 0; r0 < k; r0++) sel_msg[r0] = true;
   for (uint32_t r0 = 0; r0 < t; r0++) sel_par[r0] = true;
-  const size_t W = window_cols(n, L);
+  const size_t W = window_cols(c, n, L);
   cudaError_t e = ensure_scratch(c, (size_t)kSlots * n * W);
   if (e != cudaSuccess) return cuda_fail(e, "staging allocation");
   int slot = 0;
@@ -420,7 +548,8 @@ int afrs_encode(afrs_ctx* c, uint32_t n, uint32_t t, const uint8_t* message, uin
     const size_t w = (L - c0 < W) ? L - c0 : W;
     uint8_t* dm = c->scratch + (size_t)slot * n * W;
     uint8_t* dp = dm + (size_t)k * w;
-    const std::vector<RowRun> rm = row_runs(sel_msg, k, w), rp = row_runs(sel_par, t, w);
+    const std::vector<RowRun> rm = row_runs(sel_msg, k, w, c->merge_bytes),
+                              rp = row_runs(sel_par, t, w, c->merge_bytes);
     r = AFRS_OK;
     if ((e = cudaStreamWaitEvent(c->copy_in, c->ev_out[slot], 0)) == cudaSuccess &&
         (e = copy_rows_h2d(dm, w, message, L, c0, rm, c->copy_in)) == cudaSuccess &&
@@ -466,6 +595,22 @@ int afrs_recover(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* received, size_t 
   a.t = (int)t;
   a.e = (int)e_count;
   std::memcpy(a.pos, positions, e_count);
+  uint8_t* drx = c->direct_mode != AFRS_HOST_STAGED ? mapped_host_range(received, (size_t)n * L) : nullptr;
+  if (drx) {
+    a.rx = drx;
+    a.L = L;
+    r = run_direct(
+        c, a, [&](size_t W) { return afrs::scratch_bytes_recover((int)n, W); },
+        [](afrs::RecoverArgs& w, size_t c0) { w.rx += c0; },
+        [](const afrs::RecoverArgs& w, const afrs::ScratchArena& sc, cudaStream_t s) {
+          return afrs::launch_recover_special(w, sc, s);
+        },
+        "recover (page-locked buffers)");
+    if (r) return r;
+    g_h2d_bytes.fetch_add((uint64_t)(n - e_count) * L, std::memory_order_relaxed);
+    g_d2h_bytes.fetch_add((uint64_t)e_count * L, std::memory_order_relaxed);
+    return 1;
+  }
   r = staged(c, n, L, received, survivor, received, erased, [&](uint8_t* base, size_t w) {
     a.rx = base;
     a.L = w;

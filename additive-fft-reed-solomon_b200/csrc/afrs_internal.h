@@ -10,19 +10,25 @@ namespace afrs {
 // Parameters of one recover launch, passed by value (kernel parameter space),
 // so a launch needs no device allocation.
 struct RecoverArgs {
-  uint8_t* rx;       // n * L bytes, shard-major
-  size_t L;          // shard length
+  uint8_t* rx;       // n rows of L bytes, shard-major
+  size_t L;          // shard length (columns processed)
   int n, t, e;       // shards, parity shards, erasures
   uint8_t pos[256];  // erased positions (first e entries)
+  size_t pitch = 0;  // bytes between rows; 0 = L (the special kernels honour it)
 };
 
 struct EncodeArgs {
-  const uint8_t* msg;  // (n - t) * L
-  uint8_t* parity;     // t * L
+  const uint8_t* msg;  // (n - t) rows
+  uint8_t* parity;     // t rows
   size_t L;
   int n, t;
   int accumulate;
+  size_t pitch = 0;  // bytes between rows of msg and parity; 0 = L
 };
+template <class A>
+__host__ __device__ inline size_t row_pitch(const A& a) {
+  return a.pitch ? a.pitch : a.L;
+}
 
 // Batched launch (batch.cu): device tables built by afrs_batch_dev.
 struct BatchJob {

@@ -132,15 +132,16 @@ __device__ __forceinline__ void sstore(uint32_t* sm, int row, int w, const uint3
 }
 
 // Shard row <-> bit-sliced planes for global colword w (io.cuh layout).
-__device__ __forceinline__ void gload(const uint8_t* base, size_t row, size_t L, size_t w, uint32_t (&x)[8],
-                                      const ShiftMul& km) {
-  load_cw(base + row * L, L, w, x);
+// Row r starts at base + r * pitch; columns [0, L) exist.
+__device__ __forceinline__ void gload(const uint8_t* base, size_t row, size_t pitch, size_t L, size_t w,
+                                      uint32_t (&x)[8], const ShiftMul& km) {
+  load_cw(base + row * pitch, L, w, x);
   transpose8f(x, km);
 }
-__device__ __forceinline__ void gstore(uint8_t* base, size_t row, size_t L, size_t w, uint32_t (&x)[8],
-                                       const ShiftMul& km) {
+__device__ __forceinline__ void gstore(uint8_t* base, size_t row, size_t pitch, size_t L, size_t w,
+                                       uint32_t (&x)[8], const ShiftMul& km) {
   transpose8f(x, km);
-  store_cw(base + row * L, L, w, x);
+  store_cw(base + row * pitch, L, w, x);
 }
 
 // y <- c * y for c = g^a (g = 2), a in [0, 254] uniform across the CTA:
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
   for (int c = 1; c <= C; c++) {
     uint32_t x[T][8];
 #pragma unroll
-    for (int r = 0; r < T; r++) gload(a.msg, (size_t)(c - 1) * T + r, a.L, cw, x[r], km);
+    for (int r = 0; r < T; r++) gload(a.msg, (size_t)(c - 1) * T + r, row_pitch(a), a.L, cw, x[r], km);
     if constexpr (LOGT > 0) {
       dispatch<1, C>(c, [&](auto cc) {
         constexpr int CC = decltype(cc)::value;
@@ -234,14 +235,14 @@ __global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
       for (int p = 0; p < 8; p++) f[r][p] = acc[r][p];
     if (a.accumulate) {
       uint32_t y[8];
-      gload(a.parity, r, a.L, cw, y, km);
+      gload(a.parity, r, row_pitch(a), a.L, cw, y, km);
 #pragma unroll
       for (int p = 0; p < 8; p++) f[r][p] ^= y[p];
     }
   }
   block_fft<0, LOGT, 0, 0, T>(f);
 #pragma unroll
-  for (int r = 0; r < T; r++) gstore(a.parity, r, a.L, cw, f[r], km);
+  for (int r = 0; r < T; r++) gstore(a.parity, r, row_pitch(a), a.L, cw, f[r], km);
 }
 
 
@@ -272,72 +273,11 @@ struct Batch {
 
 constexpr int kPhaseThreads = 128;
 
-// ---- per-thread staging of 16 rows in shared memory -----------------------
-// Slot (row i, half h) of the calling thread: 16 bytes at
-// st[(i * 2 + h) * kPhaseThreads + tid] (consecutive threads, consecutive
-// 16-byte words).  Rows are fetched with cp.async (all 32 copies in flight at
-// once), transposed to planes in a rolled loop (one copy of the transpose
-// code instead of 16), then read into registers for the unrolled transform.
-// 16 rows x 32 bytes x kPhaseThreads = 64 KiB per CTA.
-constexpr size_t kStageBytes = (size_t)16 * 32 * kPhaseThreads;
-
-__device__ __forceinline__ uint4* st4(uint32_t* st, int i, int h) {
-  return reinterpret_cast<uint4*>(st) + (i * 2 + h) * kPhaseThreads + threadIdx.x;
-}
-
+// cp.async copy of 16 bytes from global (device or mapped host) memory to
+// shared memory.
 __device__ __forceinline__ void cp_async16(uint4* dst, const uint8_t* src) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-
-// Rows first_row + i (i < 16) of colword w, except those whose bit is set in
-// `skip` (staged as zero).  Runs and tails that are not 16-byte aligned and
-// in bounds take ordinary loads.
-__device__ __forceinline__ void stage_rows(uint32_t* st, const uint8_t* base, size_t first_row, size_t L, size_t w,
-                                           uint32_t skip) {
-  const size_t c = cw_col(w);
-#pragma unroll
-  for (int i = 0; i < 16; i++) {
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      uint4* dst = st4(st, i, h);
-      if ((skip >> i) & 1) {
-        *dst = make_uint4(0, 0, 0, 0);
-        continue;
-      }
-      const size_t col = c + 512 * h;
-      const uint8_t* row = base + (first_row + i) * L;
-      if (col + 16 <= L && ((reinterpret_cast<uintptr_t>(row + col) & 15) == 0)) {
-        cp_async16(dst, row + col);
-      } else {
-        uint32_t x[4];
-        load16(row, col, L, x);
-        *dst = make_uint4(x[0], x[1], x[2], x[3]);
-      }
-    }
-  }
-  asm volatile("cp.async.wait_all;" ::: "memory");
-}
-
-__device__ __forceinline__ void st_get(uint32_t* st, int i, uint32_t (&x)[8]) {
-  const uint4 a = *st4(st, i, 0), b = *st4(st, i, 1);
-  x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-  x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
-}
-__device__ __forceinline__ void st_put(uint32_t* st, int i, const uint32_t (&x)[8]) {
-  *st4(st, i, 0) = make_uint4(x[0], x[1], x[2], x[3]);
-  *st4(st, i, 1) = make_uint4(x[4], x[5], x[6], x[7]);
-}
-
-// Staged bytes of the 16 rows -> planes, in place (rolled).
-__device__ __forceinline__ void stage_to_planes(uint32_t* st, const ShiftMul& km) {
-#pragma unroll 1
-  for (int i = 0; i < 16; i++) {
-    uint32_t x[8];
-    st_get(st, i, x);
-    transpose8f(x, km);
-    st_put(st, i, x);
-  }
 }
 
 // ---- encode, t >= 32 -------------------------------------------------------
@@ -370,7 +310,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt
 #pragma unroll
     for (int m = 0; m < TR; m++) {
       uint32_t q[8];
-      gload(a.parity, b + 16 * m, a.L, bt.cw0 + w, q, km);
+      gload(a.parity, b + 16 * m, row_pitch(a), a.L, bt.cw0 + w, q, km);
 #pragma unroll
       for (int p = 0; p < 8; p++) acc[m][p] ^= q[p];
     }
@@ -406,8 +346,8 @@ __device__ __forceinline__ void s8_put(uint32_t* st, int i, int tid, const uint3
 
 // Rows first_row + i (i < 8) of colword w into the calling thread's slots
 // (cp.async where 16-byte aligned and in bounds); bit i of skip stages zero.
-__device__ __forceinline__ void stage8(uint32_t* st, const uint8_t* base, size_t first_row, size_t L, size_t w,
-                                       uint32_t skip) {
+__device__ __forceinline__ void stage8(uint32_t* st, const uint8_t* base, size_t first_row, size_t pitch, size_t L,
+                                       size_t w, uint32_t skip) {
   const size_t c = cw_col(w);
   const int tid = threadIdx.x;
 #pragma unroll
@@ -420,7 +360,7 @@ __device__ __forceinline__ void stage8(uint32_t* st, const uint8_t* base, size_t
         continue;
       }
       const size_t col = c + 512 * hf;
-      const uint8_t* row = base + (first_row + i) * L;
+      const uint8_t* row = base + (first_row + i) * pitch;
       if (col + 16 <= L && ((reinterpret_cast<uintptr_t>(row + col) & 15) == 0)) {
         cp_async16(dst, row + col);
       } else {
@@ -512,7 +452,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt
   uint32_t x[8][8];
   zero_rows(x);
   if (q.active) {
-    stage8(st, a.msg, row0, a.L, bt.cw0 + q.w, 0);
+    stage8(st, a.msg, row0, row_pitch(a), a.L, bt.cw0 + q.w, 0);
 #pragma unroll 1
     for (int i = 0; i < 8; i++) {
       uint32_t y[8];
@@ -567,7 +507,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt
     for (int i = 0; i < 8; i++) {
       uint32_t y[8];
       s8_get(st, i, threadIdx.x, y);
-      gstore(a.parity, row0 + i, a.L, bt.cw0 + q.w, y, km);
+      gstore(a.parity, row0 + i, row_pitch(a), a.L, bt.cw0 + q.w, y, km);
     }
   }
 }
@@ -598,7 +538,7 @@ __global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
 #pragma unroll
       for (int p = 0; p < 8; p++) x[r][p] = 0;
     } else {
-      gload(a.rx, r, a.L, cw, x[r], km);
+      gload(a.rx, r, row_pitch(a), a.L, cw, x[r], km);
       scale_rt(x[r], c_tab.exp[s_lam[r]]);
     }
   }
@@ -609,7 +549,7 @@ __global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
   for (int r = 0; r < N; r++) {
     if (s_er[r]) {
       scale_rt(x[r], c_tab.exp[s_ilp[r]]);
-      gstore(a.rx, r, a.L, cw, x[r], km);
+      gstore(a.rx, r, row_pitch(a), a.L, cw, x[r], km);
     }
   }
 }
@@ -709,7 +649,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch b
     uint32_t skip = 0;
 #pragma unroll
     for (int i = 0; i < 8; i++) skip |= (uint32_t)(loc.er[row0 + i] != 0) << i;
-    stage8(st, a.rx, row0, a.L, bt.cw0 + q.w, skip);
+    stage8(st, a.rx, row0, row_pitch(a), a.L, bt.cw0 + q.w, skip);
 #pragma unroll 1
     for (int i = 0; i < 8; i++) {
       if ((skip >> i) & 1) continue;
@@ -795,7 +735,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_rec_b3(RecoverArgs a, Batch b
       uint32_t y[8];
       s8_get(st, i, tid, y);
       scale_log(y, loc.ilp[r]);
-      gstore(a.rx, r, a.L, bt.cw0 + q.w, y, km);
+      gstore(a.rx, r, row_pitch(a), a.L, bt.cw0 + q.w, y, km);
     }
   }
 }

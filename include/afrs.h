@@ -150,14 +150,29 @@ int afrs_recover_dev_noalloc(uint32_t n, uint32_t t, uint8_t* d_received, size_t
 /* Library build information (kernel set, arch) for logs. */
 const char* afrs_version(void);
 
+/* How the host-buffer entry points (afrs_encode, afrs_recover) move data.
+ * Staged: copy engines move shard columns in windows of about window_bytes
+ * per codeword through device buffers (two windows in flight: copy-in,
+ * kernels and copy-out overlap); runs of copied rows closer than merge_bytes
+ * are merged into one copy.  Direct: when a buffer is page-locked and mapped,
+ * the kernels read and write it themselves (exactly the rows the operation
+ * needs).  AFRS_HOST_AUTO (default): recover direct when possible, encode
+ * staged.  window_bytes / merge_bytes 0 select the defaults (4 MiB, 128 KiB);
+ * merge_bytes = SIZE_MAX disables merging. */
+#define AFRS_HOST_AUTO 0
+#define AFRS_HOST_STAGED 1
+#define AFRS_HOST_DIRECT 2
+int afrs_ctx_set_staging(afrs_ctx* ctx, size_t window_bytes, size_t merge_bytes, int host_mode);
+
 /* Number of CUDA kernels this library has launched in this process, over
  * every context and entry point (a diagnostic for benchmarks and tests; no
  * counterpart in the reference). */
 uint64_t afrs_kernel_launches(void);
 
-/* Bytes the host-buffer entry points (afrs_encode, afrs_recover) have copied
- * host -> device and device -> host in this process (a diagnostic; no
- * counterpart in the reference). */
+/* Bytes the host-buffer entry points (afrs_encode, afrs_recover) have moved
+ * host -> device and device -> host in this process: staging copies, or the
+ * kernels' own reads and writes when the host buffers are page-locked and
+ * mapped (a diagnostic; no counterpart in the reference). */
 void afrs_staged_bytes(uint64_t* h2d, uint64_t* d2h);
 
 #ifdef __cplusplus

@@ -352,3 +352,61 @@ def test_cuda_graph_capture_and_replay(afrs, n, t, L):
     torch.cuda.synchronize()
     assert (d_par.cpu().numpy() == par).all()
     assert (d_rx.cpu().numpy() == cw).all()
+
+
+def _staged_bytes(afrs):
+    import ctypes
+
+    a, b = ctypes.c_uint64(), ctypes.c_uint64()
+    afrs.lib().afrs_staged_bytes(ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,t,L", [(256, 128, 65536), (64, 32, 1000), (16, 4, 4097)])
+def test_direct_path_for_page_locked_buffers(afrs, n, t, L):
+    """Page-locked host buffers are read and written by the kernels directly:
+    recover moves exactly the surviving shards in and the erased shards out,
+    encode the message in and the parity out; results equal the oracle's."""
+    msg, par = _codeword(n, t, L, seed=3 * n + t)
+    cw = np.concatenate([par, msg])
+    codec = afrs.Codec(n, t)
+    h_msg, h_par = _pinned(msg), _pinned(np.zeros(t * L, np.uint8))
+    b0 = _staged_bytes(afrs)
+    codec.encode_parity(h_msg, h_par, L)
+    b1 = _staged_bytes(afrs)
+    assert (h_par == par).all()
+    assert (b1[0] - b0[0], b1[1] - b0[1]) == ((n - t) * L, t * L)
+    pos = sorted(np.random.default_rng(L).choice(n, t, replace=False).tolist())
+    h_rx = _pinned(_erase(cw, L, pos))
+    assert codec.recover_erasure_shards(h_rx, None, L, pos)
+    b2 = _staged_bytes(afrs)
+    assert (h_rx == cw).all()
+    assert (b2[0] - b1[0], b2[1] - b1[1]) == ((n - len(pos)) * L, len(pos) * L)
+
+
+@pytest.mark.gpu
+def test_host_registered_buffers(afrs):
+    """Memory page-locked with cudaHostRegister (whose device alias may differ
+    from its host address) and a sub-range of a page-locked buffer."""
+    n, t, L = 128, 32, 3000
+    msg, par = _codeword(n, t, L, seed=77)
+    cw = np.concatenate([par, msg])
+    pos = list(range(10, 10 + t))
+    size = (n * L + 8192 + 4095) // 4096 * 4096
+    raw = np.zeros(size + 4096, np.uint8)
+    off = (-raw.ctypes.data) % 4096
+    big = raw[off:off + size]  # page-aligned start and size
+    view = big[4096:4096 + n * L]
+    view[:] = _erase(cw, L, pos)
+    rt = torch.cuda.cudart()
+    assert int(rt.cudaHostRegister(big.ctypes.data, big.nbytes, 0)) == 0
+    try:
+        assert afrs.Codec(n, t).recover_erasure_shards(view, None, L, pos)
+        assert (view == cw).all()
+    finally:
+        rt.cudaHostUnregister(big.ctypes.data)
+    sub = _pinned(np.zeros(n * L + 100, np.uint8))[37:37 + n * L]
+    sub[:] = _erase(cw, L, pos)
+    assert afrs.Codec(n, t).recover_erasure_shards(sub, None, L, pos)
+    assert (sub == cw).all()
