@@ -263,6 +263,25 @@ __device__ __forceinline__ void xstore(uint32_t* s, size_t ncw, int r, size_t w,
   q[(size_t)(2 * r + 1) * ncw + w] = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
+// Drops from L2, without writing them back, the scratch lines of rows
+// [r0, r0 + 8) of the calling warp's colwords [w0, w0 + 32): once the last
+// pass has read them they are dead (every operation writes its scratch before
+// it reads it), and otherwise L2 writes them back to DRAM when it evicts
+// them.  A warp owns whole lines only when its 32 colwords are all in the
+// batch and every (row, half) region starts on a 128-byte boundary (ncw a
+// multiple of 8); otherwise nothing is dropped.  Call it only after the
+// warp's loads of those rows have been consumed.
+__device__ __forceinline__ void discard_rows(const uint32_t* s, size_t ncw, int r0, size_t w0) {
+  if (ncw % 8 != 0 || w0 + 32 > ncw) return;
+  const uint4* q = reinterpret_cast<const uint4*>(s);
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = lane; k < 64; k += 32) {  // 16 regions x 4 lines of 128 bytes
+    const uint4* p = q + (size_t)(2 * r0 + (k >> 2)) * ncw + w0 + 8 * (k & 3);
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+  }
+}
+
 // One batch of colwords [cw0, cw0 + ncw) of a phase kernel.
 struct Batch {
   uint32_t* s1;  // scratch (bit-sliced rows)
@@ -496,6 +515,8 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt
     constexpr int GG = decltype(vv)::value;
     pair_fft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
   });
+  // The scratch rows were stored to shared memory before the barriers above.
+  discard_rows(bt.s1, bt.ncw, row0, q.w - (threadIdx.x & 31));
   dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
     constexpr int VV = decltype(vv)::value;
     block_fft<0, 3, VV, 0, 8>(x);
@@ -721,6 +742,10 @@ __global__ void __launch_bounds__(kSplitThreads) k_rec_b3(RecoverArgs a, Batch b
     constexpr int GG = decltype(vv)::value;
     pair_fft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
   });
+  // Both scratch buffers' rows were consumed into x, which was stored to
+  // shared memory before the barriers above.
+  discard_rows(bt.s1, bt.ncw, row0, q.w - (tid & 31));
+  discard_rows(bt.s2, bt.ncw, row0, q.w - (tid & 31));
   dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
     constexpr int VV = decltype(vv)::value;
     block_fft<0, 3, VV, 0, 8>(x);
