@@ -263,25 +263,6 @@ __device__ __forceinline__ void xstore(uint32_t* s, size_t ncw, int r, size_t w,
   q[(size_t)(2 * r + 1) * ncw + w] = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
-// Drops from L2, without writing them back, the scratch lines of rows
-// [r0, r0 + 8) of the calling warp's colwords [w0, w0 + 32): once the last
-// pass has read them they are dead (every operation writes its scratch before
-// it reads it), and otherwise L2 writes them back to DRAM when it evicts
-// them.  A warp owns whole lines only when its 32 colwords are all in the
-// batch and every (row, half) region starts on a 128-byte boundary (ncw a
-// multiple of 8); otherwise nothing is dropped.  Call it only after the
-// warp's loads of those rows have been consumed.
-__device__ __forceinline__ void discard_rows(const uint32_t* s, size_t ncw, int r0, size_t w0) {
-  if (ncw % 8 != 0 || w0 + 32 > ncw) return;
-  const uint4* q = reinterpret_cast<const uint4*>(s);
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int k = lane; k < 64; k += 32) {  // 16 regions x 4 lines of 128 bytes
-    const uint4* p = q + (size_t)(2 * r0 + (k >> 2)) * ncw + w0 + 8 * (k & 3);
-    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
-  }
-}
-
 // One batch of colwords [cw0, cw0 + ncw) of a phase kernel.
 struct Batch {
   uint32_t* s1;  // scratch (bit-sliced rows)
@@ -340,40 +321,55 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt
 }
 
 
-// ---- bottom passes split over a warp pair -------------------------------
-// A 16-row bottom group (levels 0..3) is shared by two warps of a CTA: warp
-// h of a pair holds rows 16g + 8h + i (i < 8) of the same 32 colwords.  Levels
-// 0..2 run inside each warp (a warp-uniform compile-time variant of ~12
-// butterflies: small enough for the per-sub-partition instruction cache),
-// level 3 pairs row i of warp 0 with row i of warp 1 and goes through shared
-// memory.  Half the registers of a 16-row task, so more warps per SM.
-constexpr int kSplitThreads = 128;  // two warp pairs, 64 colwords
-constexpr size_t kStage8Bytes = (size_t)8 * 32 * kSplitThreads;
+// ---- bottom passes split over several warps -------------------------------
+// A 16-row bottom group (levels 0..3) is shared by WG = 16 / RW warps of a
+// CTA: warp q of the group holds rows 16g + RW q + i (i < RW) of the same 32
+// colwords.  The LR = log2(RW) lowest levels run inside each warp (a
+// warp-uniform compile-time variant), the higher ones pair row i of warp q
+// with row i of warp q ^ 2^(j - LR) through shared memory.  Exchanges (and
+// their barriers) are CTA-uniform code; only the combine step, whose twiddle
+// depends on the warp, is dispatched per warp.  Fewer rows per warp means
+// fewer registers, less code per warp and more warps per launch, but one more
+// exchange level: RW = 4 measured slower than RW = 8 for n = 256 with 64 KiB
+// shards (encode 31.1 vs 25.7 us, recover 54.0 vs 43.8 us) and within 5 %
+// for 1-4 MiB shards.
+constexpr int kSplitThreads = 128;  // 4 warps
+constexpr int kRowsPerWarp = 8;
 
-__device__ __forceinline__ uint4* s8(uint32_t* st, int i, int hf, int tid) {
+template <int RW>
+struct Split {
+  static_assert(RW == 4 || RW == 8, "rows per warp");
+  static constexpr int WG = 16 / RW;                 // warps per row group
+  static constexpr int LR = RW == 8 ? 3 : 2;         // levels inside a warp
+  static constexpr int CW = 32 * (4 / WG);           // colwords per CTA
+  static constexpr size_t kStage = (size_t)RW * 32 * kSplitThreads;
+};
+
+__device__ __forceinline__ uint4* sl(uint32_t* st, int i, int hf, int tid) {
   return reinterpret_cast<uint4*>(st) + (i * 2 + hf) * kSplitThreads + tid;
 }
-__device__ __forceinline__ void s8_get(uint32_t* st, int i, int tid, uint32_t (&x)[8]) {
-  const uint4 a = *s8(st, i, 0, tid), b = *s8(st, i, 1, tid);
+__device__ __forceinline__ void s_get(uint32_t* st, int i, int tid, uint32_t (&x)[8]) {
+  const uint4 a = *sl(st, i, 0, tid), b = *sl(st, i, 1, tid);
   x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
   x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
 }
-__device__ __forceinline__ void s8_put(uint32_t* st, int i, int tid, const uint32_t (&x)[8]) {
-  *s8(st, i, 0, tid) = make_uint4(x[0], x[1], x[2], x[3]);
-  *s8(st, i, 1, tid) = make_uint4(x[4], x[5], x[6], x[7]);
+__device__ __forceinline__ void s_put(uint32_t* st, int i, int tid, const uint32_t (&x)[8]) {
+  *sl(st, i, 0, tid) = make_uint4(x[0], x[1], x[2], x[3]);
+  *sl(st, i, 1, tid) = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
-// Rows first_row + i (i < 8) of colword w into the calling thread's slots
+// Rows first_row + i (i < RW) of colword w into the calling thread's slots
 // (cp.async where 16-byte aligned and in bounds); bit i of skip stages zero.
-__device__ __forceinline__ void stage8(uint32_t* st, const uint8_t* base, size_t first_row, size_t pitch, size_t L,
-                                       size_t w, uint32_t skip) {
+template <int RW>
+__device__ __forceinline__ void stage_rows(uint32_t* st, const uint8_t* base, size_t first_row, size_t pitch,
+                                           size_t L, size_t w, uint32_t skip) {
   const size_t c = cw_col(w);
   const int tid = threadIdx.x;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
+  for (int i = 0; i < RW; i++) {
 #pragma unroll
     for (int hf = 0; hf < 2; hf++) {
-      uint4* dst = s8(st, i, hf, tid);
+      uint4* dst = sl(st, i, hf, tid);
       if ((skip >> i) & 1) {
         *dst = make_uint4(0, 0, 0, 0);
         continue;
@@ -392,21 +388,25 @@ __device__ __forceinline__ void stage8(uint32_t* st, const uint8_t* base, size_t
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-// Level 3 of an IFFT over the pair: (g0, g1) = (row i of warp 0, row i of
-// warp 1) -> (g0 + T*(g0 + g1), g0 + g1).  The rows are exchanged through the
-// stage; ends with a barrier after which the stage may be reused.
-template <int TW>
-__device__ __forceinline__ void pair_ifft_level3(uint32_t* st, uint32_t (&x)[8][8], int h) {
-  const int tid = threadIdx.x;
+// CTA-uniform: every thread publishes its rows in its own slots.  The leading
+// barrier orders it after all earlier reads of the stage.
+template <int RW>
+__device__ __forceinline__ void xchg_put(uint32_t* st, const uint32_t (&x)[RW][8]) {
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);
+  for (int i = 0; i < RW; i++) s_put(st, i, threadIdx.x, x[i]);
   __syncthreads();
+}
+
+// Cross-warp IFFT level: (g0, g1) = (row i of the low warp, row i of the high
+// warp) -> (g0 + T (g0 + g1), g0 + g1); H = 1 for the high warp.
+template <int TW, int H, int RW>
+__device__ __forceinline__ void combine_ifft(uint32_t* st, uint32_t (&x)[RW][8], int ptid) {
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
+  for (int i = 0; i < RW; i++) {
     uint32_t y[8];
-    s8_get(st, i, tid ^ 32, y);
-    if (h == 0) {
+    s_get(st, i, ptid, y);
+    if constexpr (H == 0) {
       uint32_t d[8];
 #pragma unroll
       for (int p = 0; p < 8; p++) d[p] = x[i][p] ^ y[p];
@@ -416,22 +416,16 @@ __device__ __forceinline__ void pair_ifft_level3(uint32_t* st, uint32_t (&x)[8][
       for (int p = 0; p < 8; p++) x[i][p] ^= y[p];
     }
   }
-  __syncthreads();
 }
 
-// Level 3 of an FFT over the pair: (a, b) -> (a + T*b, a + (T+1)*b).
-template <int TW>
-__device__ __forceinline__ void pair_fft_level3(uint32_t* st, uint32_t (&x)[8][8], int h) {
-  const int tid = threadIdx.x;
-  __syncthreads();
+// Cross-warp FFT level: (a, b) -> (a + T b, a + (T + 1) b).
+template <int TW, int H, int RW>
+__device__ __forceinline__ void combine_fft(uint32_t* st, uint32_t (&x)[RW][8], int ptid) {
 #pragma unroll
-  for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
+  for (int i = 0; i < RW; i++) {
     uint32_t y[8];
-    s8_get(st, i, tid ^ 32, y);
-    if (h == 0) {
+    s_get(st, i, ptid, y);
+    if constexpr (H == 0) {
       if constexpr (TW != 0) mul_xor_c<static_cast<uint8_t>(TW)>(x[i], y);
     } else {
       uint32_t m[8];
@@ -442,92 +436,128 @@ __device__ __forceinline__ void pair_fft_level3(uint32_t* st, uint32_t (&x)[8][8
       for (int p = 0; p < 8; p++) x[i][p] = m[p];
     }
   }
-  __syncthreads();
 }
 
-struct PairPos {
-  int h;
-  size_t w;
-  bool active;
+template <int RW>
+struct SplitPos {
+  int q;        // warp within its row group
+  size_t w;     // colword
+  bool active;  // w inside the batch
 };
-__device__ __forceinline__ PairPos pair_pos(size_t ncw) {
+template <int RW>
+__device__ __forceinline__ SplitPos<RW> split_pos(size_t ncw) {
   const int warp = threadIdx.x >> 5;
-  PairPos q;
-  q.h = warp & 1;
-  q.w = (size_t)blockIdx.x * 64 + (warp >> 1) * 32 + (threadIdx.x & 31);
-  q.active = q.w < ncw;
-  return q;
+  SplitPos<RW> p;
+  p.q = warp % Split<RW>::WG;
+  p.w = (size_t)blockIdx.x * Split<RW>::CW + (warp / Split<RW>::WG) * 32 + (threadIdx.x & 31);
+  p.active = p.w < ncw;
+  return p;
+}
+
+// Drops from L2, without writing them back, the scratch lines of rows
+// [r0, r0 + RW) of the calling warp's colwords [w0, w0 + 32): once the last
+// pass has read them they are dead (every operation writes its scratch before
+// it reads it), and otherwise L2 writes them back to DRAM when it evicts
+// them.  A warp owns whole lines only when its 32 colwords are all in the
+// batch and every (row, half) region starts on a 128-byte boundary (ncw a
+// multiple of 8); otherwise nothing is dropped.  Call it only after the
+// warp's loads of those rows have been consumed.
+template <int RW>
+__device__ __forceinline__ void discard_rows(const uint32_t* s, size_t ncw, int r0, size_t w0) {
+  if (ncw % 8 != 0 || w0 + 32 > ncw) return;
+  const uint4* q = reinterpret_cast<const uint4*>(s);
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = lane; k < 8 * RW; k += 32) {  // 2 RW regions x 4 lines of 128 bytes
+    const uint4* p = q + (size_t)(2 * r0 + (k >> 2)) * ncw + w0 + 8 * (k & 3);
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+  }
 }
 
 // E1 (split): bottom IFFT of chunk c, group g; blockIdx.y = (c - 1) * (t/16) + g.
 template <int LOGN, int LOGT>
 __global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt) {
+  constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
   extern __shared__ uint32_t st[];
-  const PairPos q = pair_pos(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
   const ShiftMul km = make_shift_mul();
   const int v = blockIdx.y, c = v / G + 1, g = v % G;
-  const size_t row0 = (size_t)(c - 1) * T + 16 * g + 8 * q.h;
-  uint32_t x[8][8];
+  const size_t row0 = (size_t)(c - 1) * T + 16 * g + RW * q.q;
+  uint32_t x[RW][8];
   zero_rows(x);
   if (q.active) {
-    stage8(st, a.msg, row0, row_pitch(a), a.L, bt.cw0 + q.w, 0);
+    stage_rows<RW>(st, a.msg, row0, row_pitch(a), a.L, bt.cw0 + q.w, 0);
 #pragma unroll 1
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < RW; i++) {
       uint32_t y[8];
-      s8_get(st, i, threadIdx.x, y);
+      s_get(st, i, threadIdx.x, y);
       transpose8f(y, km);
-      s8_put(st, i, threadIdx.x, y);
+      s_put(st, i, threadIdx.x, y);
     }
 #pragma unroll
-    for (int i = 0; i < 8; i++) s8_get(st, i, threadIdx.x, x[i]);
+    for (int i = 0; i < RW; i++) s_get(st, i, threadIdx.x, x[i]);
   }
-  dispatch<0, 2 * C * G - 1>(2 * v + q.h, [&](auto vv) {
-    constexpr int VV = decltype(vv)::value, V = VV / 2, H = VV % 2;
-    block_ifft<0, 3, 2 * (V % G) + H, omega_c((V / G + 1) * T), 8>(x);
+  const int vq = v * WG + q.q;
+  dispatch<0, C * G * WG - 1>(vq, [&](auto vv) {
+    constexpr int V = decltype(vv)::value / WG, Q = decltype(vv)::value % WG;
+    block_ifft<0, LR, (V % G) * WG + Q, omega_c((V / G + 1) * T), RW>(x);
   });
-  dispatch<0, C * G - 1>(v, [&](auto vv) {
-    constexpr int V = decltype(vv)::value;
-    pair_ifft_level3<twiddle_c(3, omega_c((V / G + 1) * T), 16 * (V % G))>(st, x, q.h);
+  static_for<4 - LR>([&](auto jj) {
+    constexpr int J = LR + decltype(jj)::value;
+    xchg_put<RW>(st, x);
+    dispatch<0, C * G * WG - 1>(vq, [&](auto vv) {
+      constexpr int V = decltype(vv)::value / WG, Q = decltype(vv)::value % WG;
+      constexpr int TW = twiddle_c(J, omega_c((V / G + 1) * T), (16 * (V % G) + RW * Q) & ~((2 << J) - 1));
+      combine_ifft<TW, (Q >> (J - LR)) & 1, RW>(st, x, threadIdx.x ^ (32 << (J - LR)));
+    });
   });
   if (q.active) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) xstore(bt.s1, bt.ncw, (int)row0 + i, q.w, x[i]);
+    for (int i = 0; i < RW; i++) xstore(bt.s1, bt.ncw, (int)row0 + i, q.w, x[i]);
   }
 }
 
 // E3 (split): bottom FFT of group g = blockIdx.y, store of parity rows.
 template <int LOGN, int LOGT>
 __global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt) {
+  constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int T = 1 << LOGT, G = T / 16;
   extern __shared__ uint32_t st[];
-  const PairPos q = pair_pos(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
   const ShiftMul km = make_shift_mul();
   const int g = blockIdx.y;
-  const int row0 = 16 * g + 8 * q.h;
-  uint32_t x[8][8];
+  const int row0 = 16 * g + RW * q.q;
+  uint32_t x[RW][8];
   zero_rows(x);
   if (q.active) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) xload(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
+    for (int i = 0; i < RW; i++) xload(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
   }
-  dispatch<0, G - 1>(g, [&](auto vv) {
-    constexpr int GG = decltype(vv)::value;
-    pair_fft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
+  const int gq = g * WG + q.q;
+  static_for<4 - LR>([&](auto jj) {
+    constexpr int J = 3 - decltype(jj)::value;
+    xchg_put<RW>(st, x);
+    dispatch<0, G * WG - 1>(gq, [&](auto vv) {
+      constexpr int GG = decltype(vv)::value / WG, Q = decltype(vv)::value % WG;
+      constexpr int TW = twiddle_c(J, 0, (16 * GG + RW * Q) & ~((2 << J) - 1));
+      combine_fft<TW, (Q >> (J - LR)) & 1, RW>(st, x, threadIdx.x ^ (32 << (J - LR)));
+    });
   });
+  __syncthreads();  // partners' reads of the stage are done
   // The scratch rows were stored to shared memory before the barriers above.
-  discard_rows(bt.s1, bt.ncw, row0, q.w - (threadIdx.x & 31));
-  dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
+  discard_rows<RW>(bt.s1, bt.ncw, row0, q.w - (threadIdx.x & 31));
+  dispatch<0, G * WG - 1>(gq, [&](auto vv) {
     constexpr int VV = decltype(vv)::value;
-    block_fft<0, 3, VV, 0, 8>(x);
+    block_fft<0, LR, VV, 0, RW>(x);
   });
   if (q.active) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) s8_put(st, i, threadIdx.x, x[i]);
+    for (int i = 0; i < RW; i++) s_put(st, i, threadIdx.x, x[i]);
 #pragma unroll 1
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < RW; i++) {
       uint32_t y[8];
-      s8_get(st, i, threadIdx.x, y);
+      s_get(st, i, threadIdx.x, y);
       gstore(a.parity, row0 + i, row_pitch(a), a.L, bt.cw0 + q.w, y, km);
     }
   }
@@ -658,107 +688,126 @@ struct GroupList {
 // R1 (split): lambda-scale + bottom IFFT of group g = blockIdx.y.
 template <int LOGN>
 __global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
+  constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int G = (1 << LOGN) / 16;
   extern __shared__ uint32_t st[];
-  const PairPos q = pair_pos(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
   const ShiftMul km = make_shift_mul();
   const int g = blockIdx.y;
-  const int row0 = 16 * g + 8 * q.h;
-  uint32_t x[8][8];
+  const int row0 = 16 * g + RW * q.q;
+  uint32_t x[RW][8];
   zero_rows(x);
   if (q.active) {
     uint32_t skip = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) skip |= (uint32_t)(loc.er[row0 + i] != 0) << i;
-    stage8(st, a.rx, row0, row_pitch(a), a.L, bt.cw0 + q.w, skip);
+    for (int i = 0; i < RW; i++) skip |= (uint32_t)(loc.er[row0 + i] != 0) << i;
+    stage_rows<RW>(st, a.rx, row0, row_pitch(a), a.L, bt.cw0 + q.w, skip);
 #pragma unroll 1
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < RW; i++) {
       if ((skip >> i) & 1) continue;
       uint32_t y[8];
-      s8_get(st, i, threadIdx.x, y);
+      s_get(st, i, threadIdx.x, y);
       transpose8f(y, km);
       scale_log(y, loc.lam[row0 + i]);
-      s8_put(st, i, threadIdx.x, y);
+      s_put(st, i, threadIdx.x, y);
     }
 #pragma unroll
-    for (int i = 0; i < 8; i++) s8_get(st, i, threadIdx.x, x[i]);
+    for (int i = 0; i < RW; i++) s_get(st, i, threadIdx.x, x[i]);
   }
-  dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
+  const int gq = g * WG + q.q;
+  dispatch<0, G * WG - 1>(gq, [&](auto vv) {
     constexpr int VV = decltype(vv)::value;
-    block_ifft<0, 3, VV, 0, 8>(x);
+    block_ifft<0, LR, VV, 0, RW>(x);
   });
-  dispatch<0, G - 1>(g, [&](auto vv) {
-    constexpr int GG = decltype(vv)::value;
-    pair_ifft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
+  static_for<4 - LR>([&](auto jj) {
+    constexpr int J = LR + decltype(jj)::value;
+    xchg_put<RW>(st, x);
+    dispatch<0, G * WG - 1>(gq, [&](auto vv) {
+      constexpr int GG = decltype(vv)::value / WG, Q = decltype(vv)::value % WG;
+      constexpr int TW = twiddle_c(J, 0, (16 * GG + RW * Q) & ~((2 << J) - 1));
+      combine_ifft<TW, (Q >> (J - LR)) & 1, RW>(st, x, threadIdx.x ^ (32 << (J - LR)));
+    });
   });
   if (q.active) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) xstore(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
+    for (int i = 0; i < RW; i++) xstore(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
   }
 }
 
 // R3 (split): x = s2 + (I + D_bot) s1 on group g, bottom FFT, Forney, store
-// the erased rows.  (I + D_bot) = (I + D_0..2) inside each warp plus, for
-// warp 0, the bit-3 term: row m gets original row m + 8 of warp 1.
+// the erased rows.  (I + D_bot) = (I + D over the in-warp bits) applied in
+// registers, plus, for each cross-warp bit j that is clear in the warp's rows,
+// the ORIGINAL row i of the warp whose rows have bit j set.
 template <int LOGN>
-__global__ void __launch_bounds__(kSplitThreads) k_rec_b3(RecoverArgs a, Batch bt, GroupList gl,
-                                                           const __grid_constant__ LocTable loc) {
+__global__ void __launch_bounds__(kSplitThreads)
+    k_rec_b3(RecoverArgs a, Batch bt, GroupList gl, const __grid_constant__ LocTable loc) {
+  constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int G = (1 << LOGN) / 16;
   extern __shared__ uint32_t st[];
-  const PairPos q = pair_pos(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
   const ShiftMul km = make_shift_mul();
   const int g = gl.g[blockIdx.y];
-  const int row0 = 16 * g + 8 * q.h;
+  const int row0 = 16 * g + RW * q.q;
   const int tid = threadIdx.x;
-  uint32_t x[8][8];
+  uint32_t x[RW][8];
   zero_rows(x);
   if (q.active) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) xload(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
+    for (int i = 0; i < RW; i++) xload(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
   }
 #pragma unroll
-  for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);  // original c' for the partner
+  for (int i = 0; i < RW; i++) s_put(st, i, tid, x[i]);  // original c' for the partners
   __syncthreads();
-  one_plus_derivative<8>(x);
-  if (q.h == 0) {
+  one_plus_derivative<RW>(x);
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+  for (int j = LR; j < 4; j++) {
+    if ((q.q >> (j - LR)) & 1) continue;
+    const int ptid = tid ^ (32 << (j - LR));
+#pragma unroll
+    for (int i = 0; i < RW; i++) {
       uint32_t y[8];
-      s8_get(st, i, tid ^ 32, y);
+      s_get(st, i, ptid, y);
 #pragma unroll
       for (int p = 0; p < 8; p++) x[i][p] ^= y[p];
     }
   }
   if (q.active) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < RW; i++) {
       uint32_t u[8];
       xload(bt.s2, bt.ncw, row0 + i, q.w, u);
 #pragma unroll
       for (int p = 0; p < 8; p++) x[i][p] ^= u[p];
     }
   }
-  dispatch<0, G - 1>(g, [&](auto vv) {
-    constexpr int GG = decltype(vv)::value;
-    pair_fft_level3<twiddle_c(3, 0, 16 * GG)>(st, x, q.h);
+  const int gq = g * WG + q.q;
+  static_for<4 - LR>([&](auto jj) {
+    constexpr int J = 3 - decltype(jj)::value;
+    xchg_put<RW>(st, x);
+    dispatch<0, G * WG - 1>(gq, [&](auto vv) {
+      constexpr int GG = decltype(vv)::value / WG, Q = decltype(vv)::value % WG;
+      constexpr int TW = twiddle_c(J, 0, (16 * GG + RW * Q) & ~((2 << J) - 1));
+      combine_fft<TW, (Q >> (J - LR)) & 1, RW>(st, x, tid ^ (32 << (J - LR)));
+    });
   });
+  __syncthreads();  // partners' reads of the stage are done
   // Both scratch buffers' rows were consumed into x, which was stored to
   // shared memory before the barriers above.
-  discard_rows(bt.s1, bt.ncw, row0, q.w - (tid & 31));
-  discard_rows(bt.s2, bt.ncw, row0, q.w - (tid & 31));
-  dispatch<0, 2 * G - 1>(2 * g + q.h, [&](auto vv) {
+  discard_rows<RW>(bt.s1, bt.ncw, row0, q.w - (tid & 31));
+  discard_rows<RW>(bt.s2, bt.ncw, row0, q.w - (tid & 31));
+  dispatch<0, G * WG - 1>(gq, [&](auto vv) {
     constexpr int VV = decltype(vv)::value;
-    block_fft<0, 3, VV, 0, 8>(x);
+    block_fft<0, LR, VV, 0, RW>(x);
   });
   if (q.active) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) s8_put(st, i, tid, x[i]);
+    for (int i = 0; i < RW; i++) s_put(st, i, tid, x[i]);
 #pragma unroll 1
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < RW; i++) {
       const int r = row0 + i;
       if (!loc.er[r]) continue;
       uint32_t y[8];
-      s8_get(st, i, tid, y);
+      s_get(st, i, tid, y);
       scale_log(y, loc.ilp[r]);
       gstore(a.rx, r, row_pitch(a), a.L, bt.cw0 + q.w, y, km);
     }
@@ -802,10 +851,12 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
     for (size_t cw0 = 0; cw0 < total_cw; cw0 += bcw) {
       Batch bt{sc.ptr, nullptr, (total_cw - cw0 < bcw ? total_cw - cw0 : bcw), cw0};
       const unsigned gx = (unsigned)((bt.ncw + kPhaseThreads - 1) / kPhaseThreads);
-      const unsigned gs = (unsigned)((bt.ncw + 63) / 64);
-      k_enc_b1<LOGN, LOGT><<<dim3(gs, C * G), kSplitThreads, kStage8Bytes, s>>>(a, bt);
+      constexpr int SCW = Split<kRowsPerWarp>::CW;
+      constexpr size_t kStage = Split<kRowsPerWarp>::kStage;
+      const unsigned gs = (unsigned)((bt.ncw + SCW - 1) / SCW);
+      k_enc_b1<LOGN, LOGT><<<dim3(gs, C * G), kSplitThreads, kStage, s>>>(a, bt);
       k_enc_p2<LOGN, LOGT><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_enc_b3<LOGN, LOGT><<<dim3(gs, G), kSplitThreads, kStage8Bytes, s>>>(a, bt);
+      k_enc_b3<LOGN, LOGT><<<dim3(gs, G), kSplitThreads, kStage, s>>>(a, bt);
       count_launches(3);
     }
     return cudaGetLastError();
@@ -836,10 +887,12 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
       const size_t ncw = total_cw - cw0 < bcw ? total_cw - cw0 : bcw;
       Batch bt{sc.ptr, sc.ptr + (size_t)N * ncw * 8, ncw, cw0};
       const unsigned gx = (unsigned)((ncw + kPhaseThreads - 1) / kPhaseThreads);
-      const unsigned gs = (unsigned)((ncw + 63) / 64);
-      k_rec_b1<LOGN><<<dim3(gs, G), kSplitThreads, kStage8Bytes, s>>>(a, bt, loc);
+      constexpr int SCW = Split<kRowsPerWarp>::CW;
+      constexpr size_t kStage = Split<kRowsPerWarp>::kStage;
+      const unsigned gs = (unsigned)((ncw + SCW - 1) / SCW);
+      k_rec_b1<LOGN><<<dim3(gs, G), kSplitThreads, kStage, s>>>(a, bt, loc);
       k_rec_p2<LOGN><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_rec_b3<LOGN><<<dim3(gs, gl.count), kSplitThreads, kStage8Bytes, s>>>(a, bt, gl, loc);
+      k_rec_b3<LOGN><<<dim3(gs, gl.count), kSplitThreads, kStage, s>>>(a, bt, gl, loc);
       count_launches(3);
     }
     return cudaGetLastError();
