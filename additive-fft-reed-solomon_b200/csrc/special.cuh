@@ -23,6 +23,8 @@
 // most, largely L2-resident); long shards are processed in column batches.
 // Transforms with k <= 4 run entirely inside one thread.
 #pragma once
+#include <utility>
+
 #include "afrs_internal.h"
 #include "gf_device.cuh"
 #include "io.cuh"
@@ -273,6 +275,16 @@ struct Batch {
 
 constexpr int kPhaseThreads = 128;
 
+// Programmatic dependent launch inside one operation: b1 and p2 let the next
+// kernel be scheduled once every CTA has finished its arithmetic (just before
+// its final stores), which hides the launch gap; p2 and b3 block in
+// griddep_wait() until the previous kernel has completed and its writes are
+// visible (a no-op when a kernel is launched without the attribute).  A
+// trigger at kernel entry measured slower when two operations share the GPU:
+// the early-scheduled CTAs hold SM slots while they wait.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // cp.async copy of 16 bytes from global (device or mapped host) memory to
 // shared memory.
 __device__ __forceinline__ void cp_async16(uint4* dst, const uint8_t* src) {
@@ -287,6 +299,7 @@ __device__ __forceinline__ void cp_async16(uint4* dst, const uint8_t* src) {
 template <int LOGN, int LOGT>
 __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt) {
   constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, TL = LOGT - 4, TR = 1 << TL;
+  griddep_wait();
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
   const int b = blockIdx.y;
@@ -316,6 +329,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt
     }
   }
   block_fft<4, TL, 0, 0, TR>(acc);
+  griddep_trigger();
 #pragma unroll
   for (int m = 0; m < TR; m++) xstore(bt.s1, bt.ncw, b + 16 * m, w, acc[m]);
 }
@@ -512,6 +526,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt
       combine_ifft<TW, (Q >> (J - LR)) & 1, RW>(st, x, threadIdx.x ^ (32 << (J - LR)));
     });
   });
+  griddep_trigger();
   if (q.active) {
 #pragma unroll
     for (int i = 0; i < RW; i++) xstore(bt.s1, bt.ncw, (int)row0 + i, q.w, x[i]);
@@ -521,6 +536,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt
 // E3 (split): bottom FFT of group g = blockIdx.y, store of parity rows.
 template <int LOGN, int LOGT>
 __global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt) {
+  griddep_wait();
   constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int T = 1 << LOGT, G = T / 16;
   extern __shared__ uint32_t st[];
@@ -665,6 +681,7 @@ inline void host_locator(const RecoverArgs& a, LocTable* t) {
 template <int LOGN>
 __global__ void __launch_bounds__(kPhaseThreads) k_rec_p2(RecoverArgs a, Batch bt) {
   constexpr int TL = LOGN - 4, TR = 1 << TL;
+  griddep_wait();
   const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
   const int b = blockIdx.y;
@@ -674,6 +691,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_rec_p2(RecoverArgs a, Batch b
   block_ifft<4, TL, 0, 0, TR>(y);
   one_plus_derivative<TR>(y);
   block_fft<4, TL, 0, 0, TR>(y);
+  griddep_trigger();
 #pragma unroll
   for (int m = 0; m < TR; m++) xstore(bt.s2, bt.ncw, b + 16 * m, w, y[m]);
 }
@@ -728,6 +746,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch b
       combine_ifft<TW, (Q >> (J - LR)) & 1, RW>(st, x, threadIdx.x ^ (32 << (J - LR)));
     });
   });
+  griddep_trigger();
   if (q.active) {
 #pragma unroll
     for (int i = 0; i < RW; i++) xstore(bt.s1, bt.ncw, row0 + i, q.w, x[i]);
@@ -741,6 +760,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch b
 template <int LOGN>
 __global__ void __launch_bounds__(kSplitThreads)
     k_rec_b3(RecoverArgs a, Batch bt, GroupList gl, const __grid_constant__ LocTable loc) {
+  griddep_wait();
   constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int G = (1 << LOGN) / 16;
   extern __shared__ uint32_t st[];
@@ -816,6 +836,25 @@ __global__ void __launch_bounds__(kSplitThreads)
 
 // ---- launchers ------------------------------------------------------------
 
+// Launch that may start before the previous kernel on the stream has
+// finished (programmatic stream serialization); the kernel must begin with
+// griddep_wait() before it touches that kernel's output.
+template <class... KArgs, class... Args>
+cudaError_t launch_dependent(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
 // Scratch budget per phase batch: both buffers together stay well inside L2.
 constexpr size_t kScratchBudget = (size_t)128 << 20;
 
@@ -855,8 +894,10 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
       constexpr size_t kStage = Split<kRowsPerWarp>::kStage;
       const unsigned gs = (unsigned)((bt.ncw + SCW - 1) / SCW);
       k_enc_b1<LOGN, LOGT><<<dim3(gs, C * G), kSplitThreads, kStage, s>>>(a, bt);
-      k_enc_p2<LOGN, LOGT><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_enc_b3<LOGN, LOGT><<<dim3(gs, G), kSplitThreads, kStage, s>>>(a, bt);
+      cudaError_t e = launch_dependent(k_enc_p2<LOGN, LOGT>, dim3(gx, 16), dim3(kPhaseThreads), 0, s, a, bt);
+      if (e == cudaSuccess)
+        e = launch_dependent(k_enc_b3<LOGN, LOGT>, dim3(gs, G), dim3(kSplitThreads), kStage, s, a, bt);
+      if (e != cudaSuccess) return e;
       count_launches(3);
     }
     return cudaGetLastError();
@@ -891,8 +932,10 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
       constexpr size_t kStage = Split<kRowsPerWarp>::kStage;
       const unsigned gs = (unsigned)((ncw + SCW - 1) / SCW);
       k_rec_b1<LOGN><<<dim3(gs, G), kSplitThreads, kStage, s>>>(a, bt, loc);
-      k_rec_p2<LOGN><<<dim3(gx, 16), kPhaseThreads, 0, s>>>(a, bt);
-      k_rec_b3<LOGN><<<dim3(gs, gl.count), kSplitThreads, kStage, s>>>(a, bt, gl, loc);
+      cudaError_t e = launch_dependent(k_rec_p2<LOGN>, dim3(gx, 16), dim3(kPhaseThreads), 0, s, a, bt);
+      if (e == cudaSuccess)
+        e = launch_dependent(k_rec_b3<LOGN>, dim3(gs, gl.count), dim3(kSplitThreads), kStage, s, a, bt, gl, loc);
+      if (e != cudaSuccess) return e;
       count_launches(3);
     }
     return cudaGetLastError();
