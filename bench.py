@@ -59,27 +59,47 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.lines = []  # (perf_counter when read, line)
+        self.window = (None, None)
 
     def start(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return
+
+        def read():
+            for line in self.proc.stdout:
+                self.lines.append((time.perf_counter(), line))
+
+        self.reader = threading.Thread(target=read, daemon=True)
+        self.reader.start()
+
+    def mark(self, begin: bool):
+        """Marks the start or the end of the timed region (host clock)."""
+        b, e = self.window
+        self.window = (time.perf_counter(), e) if begin else (b, time.perf_counter())
 
     def stop(self):
         if self.proc is None:
             return None
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-            out, _ = self.proc.communicate()
+        self.reader.join(timeout=5)
+        b, e = self.window
+        inside = [ln for ts, ln in self.lines if b is not None and e is not None and b <= ts <= e + 0.15]
+        rows = inside or [ln for _, ln in self.lines]
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for line in rows:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -93,7 +113,8 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "in_timed_region": bool(inside)}
 
 
 def cpu_baseline(seconds: float, threads: int):
@@ -111,6 +132,24 @@ def cpu_baseline(seconds: float, threads: int):
     combined = 2.0 / (1.0 / enc + 1.0 / rec)  # same mix as one GPU step: one encode + one recover
     sample = f"{iters} encodes + {iters} recovers of one n=256 t=128 L=64KiB codeword per thread, {threads} threads"
     return combined / 1e9, enc / 1e9, rec / 1e9, sample
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of one number over all ranks (the slowest rank's time);
+    every rank takes part and gets the result."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_gbs(bytes_per_rank_step: float, world: int, steps: int, max_seconds: float) -> float:
+    """Whole-job throughput: all ranks' bytes over the slowest rank's time."""
+    return world * bytes_per_rank_step * steps / max_seconds / 1e9
 
 
 def run_reference(args):
@@ -146,7 +185,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="afrs", choices=["afrs", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
@@ -276,6 +315,7 @@ def main():
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     launches0 = afrs.lib().afrs_kernel_launches()
+    clocks.mark(True)
     start.record(stream)
     s_enc.wait_stream(stream)
     s_rec.wait_stream(stream)
@@ -288,6 +328,7 @@ def main():
     if use_graphs:
         launches = int(round(launches_per_step * args.steps))  # kernel nodes replayed
     torch.cuda.synchronize()
+    clocks.mark(False)
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
@@ -296,13 +337,10 @@ def main():
     elapsed_ms = start.elapsed_time(end)
     enc_ms = [e[0].elapsed_time(e[1]) for e in evs]
     rec_ms = [e[2].elapsed_time(e[3]) for e in evs]
-    if world > 1:
-        tt = torch.tensor([elapsed_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(tt.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, world, dev)
 
     ms_per_step = elapsed_ms / args.steps
-    value = world * 2 * op_bytes / (ms_per_step * 1e-3) / 1e9
+    value = aggregate_gbs(2 * op_bytes, world, args.steps, elapsed_ms * 1e-3)
     enc_avg, rec_avg = statistics.mean(enc_ms), statistics.mean(rec_ms)
     peak, peak_kind = measured_peak_gbs()
     dom = "recover" if rec_avg >= enc_avg else "encode"
@@ -362,7 +400,8 @@ def main():
     s1 = staged()
     if pool is not None:
         pool.shutdown()
-    e2e_value = world * 2 * op_bytes * e2e_steps / e2e_time / 1e9
+    e2e_time = max_over_ranks(e2e_time, world, dev)
+    e2e_value = aggregate_gbs(2 * op_bytes, world, e2e_steps, e2e_time)
     h2d_step, d2h_step = (s1[0] - s0[0]) // e2e_steps, (s1[1] - s0[1]) // e2e_steps
 
     cpu = None
