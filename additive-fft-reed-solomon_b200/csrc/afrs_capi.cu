@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "../../include/afrs.h"
@@ -28,6 +29,12 @@ struct afrs_ctx {
   uint8_t* batch_host[2];  // pinned staging of those tables
   size_t batch_host_bytes[2];
   cudaEvent_t batch_free[2];  // recorded after each batch of the slot
+  uint32_t* grp_scratch[2];   // scratch of the slot's grouped launches
+  size_t grp_scratch_bytes[2];
+  // Streams on which the shape groups of a batch run concurrently, forked
+  // from and joined back into the caller's stream.
+  cudaStream_t grp_stream[4];
+  cudaEvent_t grp_fork, grp_join[4];
   int batch_slot;
   // Staged host-buffer path: copy streams and per-slot events.
   cudaStream_t copy_in, copy_out;
@@ -415,6 +422,8 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
     c->batch_dev_bytes[i] = 0;
     c->batch_host[i] = nullptr;
     c->batch_host_bytes[i] = 0;
+    c->grp_scratch[i] = nullptr;
+    c->grp_scratch_bytes[i] = 0;
   }
   c->batch_slot = 0;
   c->window_bytes = kWindowBytes;
@@ -434,6 +443,11 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_out[i], cudaEventDisableTiming);
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->grp_fork, cudaEventDisableTiming);
+  for (int i = 0; i < 4 && e == cudaSuccess; i++) {
+    e = cudaStreamCreateWithFlags(&c->grp_stream[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->grp_join[i], cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     cudaStreamDestroy(c->stream);
@@ -453,6 +467,7 @@ void afrs_ctx_destroy(afrs_ctx* c) {
   for (int i = 0; i < 2; i++) {
     if (c->batch_dev[i]) cudaFree(c->batch_dev[i]);
     if (c->batch_host[i]) cudaFreeHost(c->batch_host[i]);
+    if (c->grp_scratch[i]) cudaFree(c->grp_scratch[i]);
     cudaEventDestroy(c->batch_free[i]);
   }
   cudaEventDestroy(c->work_free);
@@ -462,6 +477,11 @@ void afrs_ctx_destroy(afrs_ctx* c) {
     cudaEventDestroy(c->ev_out[i]);
   }
   cudaStreamDestroy(c->copy_in);
+  for (int i = 0; i < 4; i++) {
+    cudaStreamDestroy(c->grp_stream[i]);
+    cudaEventDestroy(c->grp_join[i]);
+  }
+  cudaEventDestroy(c->grp_fork);
   cudaStreamDestroy(c->copy_out);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -692,6 +712,17 @@ int afrs_scale_dev(afrs_ctx* c, const uint8_t* src, uint8_t* dst, size_t len, ui
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// Scratch of one batch slot's grouped launches; jobs beyond it take the
+// generic persistent kernel.
+constexpr size_t kGroupScratchCap = (size_t)1 << 30;
+
+// A job of a batch that runs through the grouped phase kernels.
+struct GroupedJob {
+  size_t job;      // index into the caller's array
+  int op, n, t;    // shape key
+  size_t scratch;  // byte offset in the slot's grouped scratch
+};
+
 int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
   if (count && !jobs) return fail(AFRS_EINVAL, "jobs is NULL");
@@ -700,6 +731,8 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   std::vector<uint2> tasks;
   std::vector<int> rec;
   std::vector<uint8_t> pos;
+  std::vector<GroupedJob> grouped;
+  size_t grp_bytes = 0;
   int max_rows = 0;
   for (size_t i = 0; i < count; i++) {
     afrs_job& j = jobs[i];
@@ -730,11 +763,23 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
       }
       if (!j.src || !j.dst) continue;
     }
+    j.status = enc ? 0 : 1;
+    // Phase-kernel shapes run grouped by shape while the slot's scratch lasts.
+    const int op = enc ? 0 : 1;
+    if (afrs::jobs_supported(op, (int)j.n, (int)j.t)) {
+      const size_t need = align256(afrs::job_scratch_bytes(op, (int)j.n, (int)j.t, j.shard_len));
+      if (grp_bytes + need <= kGroupScratchCap) {
+        // Recover kernels do not depend on t: one group per n.
+        grouped.push_back(GroupedJob{i, op, (int)j.n, enc ? (int)j.t : 0, grp_bytes});
+        grp_bytes += need;
+        continue;
+      }
+    }
     afrs::BatchJob b{};
     b.src = j.src;
     b.dst = j.dst;
     b.L = j.shard_len;
-    b.op = enc ? 0 : 1;
+    b.op = op;
     b.n = (int)j.n;
     b.t = (int)j.t;
     b.e = (int)j.e;
@@ -749,16 +794,36 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
     }
     const size_t tiles = afrs::batch_tiles(j.shard_len);
     for (size_t q = 0; q < tiles; q++) tasks.push_back(make_uint2((unsigned)bj.size(), (unsigned)q));
-    j.status = enc ? 0 : 1;
     bj.push_back(b);
   }
   if (tasks.size() > (size_t)INT32_MAX) return fail(AFRS_EINVAL, "too many tiles");
-  if (bj.empty()) return AFRS_OK;
+  if (bj.empty() && grouped.empty()) return AFRS_OK;
+  // Groups of one shape, in order of first appearance; descriptors of a
+  // group form one array.
+  std::stable_sort(grouped.begin(), grouped.end(), [](const GroupedJob& x, const GroupedJob& y) {
+    return std::make_tuple(x.op, x.n, x.t) < std::make_tuple(y.op, y.n, y.t);
+  });
+  struct Group {
+    int op, n, t;
+    size_t first, count, desc_off, max_ncw;
+  };
+  std::vector<Group> groups;
   const size_t o_jobs = 0;
   const size_t o_tasks = align256(o_jobs + bj.size() * sizeof(afrs::BatchJob));
   const size_t o_rec = align256(o_tasks + tasks.size() * sizeof(uint2));
   const size_t o_pos = align256(o_rec + rec.size() * sizeof(int));
-  const size_t o_cnt = align256(o_pos + pos.size() + 1);
+  size_t o_grp = align256(o_pos + pos.size() + 1);
+  for (size_t q = 0; q < grouped.size(); q++) {
+    const GroupedJob& g = grouped[q];
+    if (groups.empty() || groups.back().op != g.op || groups.back().n != g.n || groups.back().t != g.t) {
+      if (!groups.empty()) o_grp = align256(o_grp + groups.back().count * afrs::job_desc_bytes(groups.back().op));
+      groups.push_back(Group{g.op, g.n, g.t, q, 0, o_grp, 0});
+    }
+    groups.back().count++;
+    groups.back().max_ncw = std::max(groups.back().max_ncw, afrs::job_colwords(jobs[g.job].shard_len));
+  }
+  if (!groups.empty()) o_grp = align256(o_grp + groups.back().count * afrs::job_desc_bytes(groups.back().op));
+  const size_t o_cnt = o_grp;
   const size_t upload = o_cnt;  // the locator table and the counter are written on the device
   const size_t o_loc = align256(o_cnt + sizeof(unsigned));
   const size_t total = align256(o_loc + rec.size() * 768);
@@ -767,7 +832,7 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int slot = c->batch_slot;
   c->batch_slot ^= 1;
-  // The slot's previous batch must be done with its staging and tables.
+  // The slot's previous batch must be done with its staging, tables and scratch.
   cudaError_t e = cudaEventSynchronize(c->batch_free[slot]);
   if (e != cudaSuccess) return cuda_fail(e, "batch wait");
   if (total > c->batch_dev_bytes[slot]) {
@@ -784,25 +849,85 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
     if ((e = cudaMallocHost(&c->batch_host[slot], upload * 2)) != cudaSuccess) return cuda_fail(e, "batch staging");
     c->batch_host_bytes[slot] = upload * 2;
   }
+  if (grp_bytes > c->grp_scratch_bytes[slot]) {
+    if (c->grp_scratch[slot]) cudaFree(c->grp_scratch[slot]);
+    c->grp_scratch[slot] = nullptr;
+    c->grp_scratch_bytes[slot] = 0;
+    const size_t want = std::min(kGroupScratchCap, grp_bytes * 2);
+    if ((e = cudaMalloc(reinterpret_cast<void**>(&c->grp_scratch[slot]), want)) != cudaSuccess)
+      return cuda_fail(e, "batch scratch");
+    c->grp_scratch_bytes[slot] = want;
+  }
   uint8_t* h = c->batch_host[slot];
-  std::memcpy(h + o_jobs, bj.data(), bj.size() * sizeof(afrs::BatchJob));
-  std::memcpy(h + o_tasks, tasks.data(), tasks.size() * sizeof(uint2));
+  if (!bj.empty()) std::memcpy(h + o_jobs, bj.data(), bj.size() * sizeof(afrs::BatchJob));
+  if (!tasks.empty()) std::memcpy(h + o_tasks, tasks.data(), tasks.size() * sizeof(uint2));
   if (!rec.empty()) std::memcpy(h + o_rec, rec.data(), rec.size() * sizeof(int));
   if (!pos.empty()) std::memcpy(h + o_pos, pos.data(), pos.size());
+  uint8_t* scratch = reinterpret_cast<uint8_t*>(c->grp_scratch[slot]);
+  for (const Group& gr : groups) {
+    const size_t sz = afrs::job_desc_bytes(gr.op);
+    for (size_t q = 0; q < gr.count; q++) {
+      const GroupedJob& gj = grouped[gr.first + q];
+      const afrs_job& j = jobs[gj.job];
+      uint32_t* sc = reinterpret_cast<uint32_t*>(scratch + gj.scratch);
+      void* desc = h + gr.desc_off + q * sz;
+      if (gr.op == 0) {
+        afrs::EncodeArgs a{j.src, j.dst, j.shard_len, (int)j.n, (int)j.t, 0};
+        afrs::fill_enc_job(desc, a, sc);
+      } else {
+        afrs::RecoverArgs a{};
+        a.rx = j.dst;
+        a.L = j.shard_len;
+        a.n = (int)j.n;
+        a.t = (int)j.t;
+        a.e = (int)j.e;
+        std::memcpy(a.pos, j.positions, j.e);
+        afrs::fill_rec_job(desc, a, sc);
+      }
+    }
+  }
   uint8_t* d = c->batch_dev[slot];
   if ((e = cudaMemcpyAsync(d, h, upload, cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return cuda_fail(e, "batch upload");
-  afrs::BatchLaunch bl{};
-  bl.jobs = reinterpret_cast<const afrs::BatchJob*>(d + o_jobs);
-  bl.tasks = reinterpret_cast<const uint2*>(d + o_tasks);
-  bl.ntasks = (int)tasks.size();
-  bl.rec_jobs = reinterpret_cast<const int*>(d + o_rec);
-  bl.nrec = (int)rec.size();
-  bl.pos_tab = d + o_pos;
-  bl.loc_tab = d + o_loc;
-  bl.counter = reinterpret_cast<unsigned*>(d + o_cnt);
-  bl.max_rows = max_rows;
-  if ((e = afrs::launch_batch(bl, s)) != cudaSuccess) return cuda_fail(e, "batch launch");
+  if (!bj.empty()) {
+    afrs::BatchLaunch bl{};
+    bl.jobs = reinterpret_cast<const afrs::BatchJob*>(d + o_jobs);
+    bl.tasks = reinterpret_cast<const uint2*>(d + o_tasks);
+    bl.ntasks = (int)tasks.size();
+    bl.rec_jobs = reinterpret_cast<const int*>(d + o_rec);
+    bl.nrec = (int)rec.size();
+    bl.pos_tab = d + o_pos;
+    bl.loc_tab = d + o_loc;
+    bl.counter = reinterpret_cast<unsigned*>(d + o_cnt);
+    bl.max_rows = max_rows;
+    if ((e = afrs::launch_batch(bl, s)) != cudaSuccess) return cuda_fail(e, "batch launch");
+  }
+  // Shape groups are independent: largest first, round-robin over the group
+  // streams, after the upload, joined back into `s`.
+  std::vector<size_t> order(groups.size());
+  for (size_t q = 0; q < order.size(); q++) order[q] = q;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+    return groups[x].count * groups[x].max_ncw * groups[x].n > groups[y].count * groups[y].max_ncw * groups[y].n;
+  });
+  const int nstreams = (int)std::min<size_t>(4, groups.size());
+  if (nstreams && (e = cudaEventRecord(c->grp_fork, s)) != cudaSuccess) return cuda_fail(e, "batch fork");
+  for (int k = 0; k < nstreams; k++)
+    if ((e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_fork, 0)) != cudaSuccess) return cuda_fail(e, "batch fork");
+  cudaError_t le = cudaSuccess;
+  for (size_t q = 0; q < order.size() && le == cudaSuccess; q++) {
+    const Group& gr = groups[order[q]];
+    cudaStream_t gs = c->grp_stream[q % nstreams];
+    le = gr.op == 0 ? afrs::launch_encode_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs)
+                    : afrs::launch_recover_jobs(gr.n, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
+  }
+  // Join every forked stream, also after a failed launch.
+  for (int k = 0; k < nstreams; k++) {
+    cudaError_t je = cudaEventRecord(c->grp_join[k], c->grp_stream[k]);
+    if (je == cudaSuccess) je = cudaStreamWaitEvent(s, c->grp_join[k], 0);
+    if (e == cudaSuccess) e = je;
+  }
+  if (le != cudaSuccess) return cuda_fail(le, "batch group launch");
+  if (e != cudaSuccess) return cuda_fail(e, "batch join");
   if ((e = cudaEventRecord(c->batch_free[slot], s)) != cudaSuccess) return cuda_fail(e, "batch record");
   return AFRS_OK;
 }

@@ -87,4 +87,19 @@ void set_last_error(const char* msg);
 void count_launches(unsigned k);
 size_t scratch_bytes_recover(int n, size_t L);
 
+// Grouped launches of many codewords of one shape (afrs_batch_dev): op 0 =
+// encode, 1 = recover.  Each codeword gets a descriptor (job_desc_bytes,
+// filled on the host) and its own scratch (job_scratch_bytes, the whole
+// shard width); the descriptors are copied to device memory and launched per
+// shape group.  Supported for the phase-kernel shapes (encode t >= 32,
+// recover n >= 32).
+bool jobs_supported(int op, int n, int t);
+size_t job_desc_bytes(int op);
+size_t job_scratch_bytes(int op, int n, int t, size_t L);
+size_t job_colwords(size_t L);
+void fill_enc_job(void* desc, const EncodeArgs& a, uint32_t* scratch);
+void fill_rec_job(void* desc, const RecoverArgs& a, uint32_t* scratch);
+cudaError_t launch_encode_jobs(int n, int t, const void* d_jobs, int count, size_t max_ncw, cudaStream_t s);
+cudaError_t launch_recover_jobs(int n, void* d_jobs, int count, size_t max_ncw, cudaStream_t s);
+
 }  // namespace afrs

@@ -182,12 +182,11 @@ __device__ __forceinline__ void zero_rows(uint32_t (&x)[NR][8]) {
 // codec.rs:241-265: parity = FFT_t(parity_in? ^ sum_c IFFT_t(chunk c, omega_ct), 0),
 // chunk c = message shards (c-1)t .. ct-1, c = 1 .. n/t - 1.
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
+__device__ __forceinline__ void enc_small_body(const EncodeArgs& a, unsigned bx, uint32_t* sm) {
   constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1;
   constexpr bool kSmemAcc = (T == 16);
-  extern __shared__ uint32_t sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t slice = (size_t)blockIdx.x * (kThreads / 32) + warp;
+  const size_t slice = (size_t)bx * (kThreads / 32) + warp;
   if (slice * 1024 >= a.L) return;
   const size_t cw = slice * 32 + lane;
   const ShiftMul km = make_shift_mul();
@@ -293,16 +292,22 @@ __device__ __forceinline__ void cp_async16(uint4* dst, const uint8_t* src) {
 }
 
 // ---- encode, t >= 32 -------------------------------------------------------
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
+  extern __shared__ uint32_t sm[];
+  enc_small_body<LOGN, LOGT>(a, blockIdx.x, sm);
+}
+
 // E2: top levels for rows {b + 16 m} (b = blockIdx.y): IFFT top of every
 // chunk, accumulated, plus parity_in, then FFT top at 0; written to scratch
 // rows b + 16 m (chunk 1's rows, read above by this thread only).
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt) {
+__device__ __forceinline__ void enc_p2_body(const EncodeArgs& a, const Batch& bt, unsigned bx, int by) {
   constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, TL = LOGT - 4, TR = 1 << TL;
   griddep_wait();
-  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  const size_t w = (size_t)bx * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
-  const int b = blockIdx.y;
+  const int b = by;
   uint32_t acc[TR][8];
   zero_rows(acc);
   for (int c = 1; c <= C; c++) {
@@ -332,6 +337,10 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt
   griddep_trigger();
 #pragma unroll
   for (int m = 0; m < TR; m++) xstore(bt.s1, bt.ncw, b + 16 * m, w, acc[m]);
+}
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kPhaseThreads) k_enc_p2(EncodeArgs a, Batch bt) {
+  enc_p2_body<LOGN, LOGT>(a, bt, blockIdx.x, blockIdx.y);
 }
 
 
@@ -459,11 +468,11 @@ struct SplitPos {
   bool active;  // w inside the batch
 };
 template <int RW>
-__device__ __forceinline__ SplitPos<RW> split_pos(size_t ncw) {
+__device__ __forceinline__ SplitPos<RW> split_pos(size_t ncw, unsigned bx) {
   const int warp = threadIdx.x >> 5;
   SplitPos<RW> p;
   p.q = warp % Split<RW>::WG;
-  p.w = (size_t)blockIdx.x * Split<RW>::CW + (warp / Split<RW>::WG) * 32 + (threadIdx.x & 31);
+  p.w = (size_t)bx * Split<RW>::CW + (warp / Split<RW>::WG) * 32 + (threadIdx.x & 31);
   p.active = p.w < ncw;
   return p;
 }
@@ -490,13 +499,12 @@ __device__ __forceinline__ void discard_rows(const uint32_t* s, size_t ncw, int 
 
 // E1 (split): bottom IFFT of chunk c, group g; blockIdx.y = (c - 1) * (t/16) + g.
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt) {
+__device__ __forceinline__ void enc_b1_body(const EncodeArgs& a, const Batch& bt, unsigned bx, int by, uint32_t* st) {
   constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
-  extern __shared__ uint32_t st[];
-  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw, bx);
   const ShiftMul km = make_shift_mul();
-  const int v = blockIdx.y, c = v / G + 1, g = v % G;
+  const int v = by, c = v / G + 1, g = v % G;
   const size_t row0 = (size_t)(c - 1) * T + 16 * g + RW * q.q;
   uint32_t x[RW][8];
   zero_rows(x);
@@ -535,14 +543,13 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt
 
 // E3 (split): bottom FFT of group g = blockIdx.y, store of parity rows.
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt) {
+__device__ __forceinline__ void enc_b3_body(const EncodeArgs& a, const Batch& bt, unsigned bx, int by, uint32_t* st) {
   griddep_wait();
   constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int T = 1 << LOGT, G = T / 16;
-  extern __shared__ uint32_t st[];
-  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw, bx);
   const ShiftMul km = make_shift_mul();
-  const int g = blockIdx.y;
+  const int g = by;
   const int row0 = 16 * g + RW * q.q;
   uint32_t x[RW][8];
   zero_rows(x);
@@ -579,6 +586,54 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt
   }
 }
 
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt) {
+  extern __shared__ uint32_t st[];
+  enc_b1_body<LOGN, LOGT>(a, bt, blockIdx.x, blockIdx.y, st);
+}
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt) {
+  extern __shared__ uint32_t st[];
+  enc_b3_body<LOGN, LOGT>(a, bt, blockIdx.x, blockIdx.y, st);
+}
+
+// Grouped launches (afrs_batch_dev): many codewords of one shape, codeword
+// blockIdx.z, each with its own scratch holding its whole shard width.
+// Blocks beyond a codeword's colwords leave before any barrier.
+struct EncJob {
+  EncodeArgs a;
+  uint32_t* s1;
+  size_t ncw;
+};
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kSplitThreads) k_enc_b1_jobs(const EncJob* __restrict__ jobs) {
+  extern __shared__ uint32_t st[];
+  const EncJob& j = jobs[blockIdx.z];
+  if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw) return;
+  enc_b1_body<LOGN, LOGT>(j.a, Batch{j.s1, nullptr, j.ncw, 0}, blockIdx.x, blockIdx.y, st);
+}
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kPhaseThreads) k_enc_p2_jobs(const EncJob* __restrict__ jobs) {
+  const EncJob& j = jobs[blockIdx.z];
+  enc_p2_body<LOGN, LOGT>(j.a, Batch{j.s1, nullptr, j.ncw, 0}, blockIdx.x, blockIdx.y);
+}
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kSplitThreads) k_enc_b3_jobs(const EncJob* __restrict__ jobs) {
+  extern __shared__ uint32_t st[];
+  const EncJob& j = jobs[blockIdx.z];
+  if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw) return;
+  enc_b3_body<LOGN, LOGT>(j.a, Batch{j.s1, nullptr, j.ncw, 0}, blockIdx.x, blockIdx.y, st);
+}
+
+// Grouped t <= 16 encode: one warp per 1024-column slice of codeword blockIdx.z.
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kThreads) k_enc_small_jobs(const EncJob* __restrict__ jobs) {
+  extern __shared__ uint32_t sm[];
+  const EncJob& j = jobs[blockIdx.z];
+  if ((size_t)blockIdx.x * (kThreads / 32) * 1024 >= j.a.L) return;
+  enc_small_body<LOGN, LOGT>(j.a, blockIdx.x, sm);
+}
+
 // ---- recover ------------------------------------------------------------
 // Leopard-form decoder (the same map as rs/src/codec.rs:479-569 on every
 // input whose erased rows are zero): y = lambda .* r over survivors,
@@ -588,13 +643,13 @@ __global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt
 
 // n <= 16: one warp per 1024-column slice, the whole codeword column in registers.
 template <int LOGN>
-__global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
+__device__ __forceinline__ void rec_small_body(const RecoverArgs& a, unsigned bx) {
   constexpr int N = 1 << LOGN;
   __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
   if (threadIdx.x < 32) erasure_locator_warp(a, c_tab, s_er, s_lam, s_ilp);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t slice = (size_t)blockIdx.x * (kThreads / 32) + warp;
+  const size_t slice = (size_t)bx * (kThreads / 32) + warp;
   if (slice * 1024 >= a.L) return;
   const size_t cw = slice * 32 + lane;
   const ShiftMul km = make_shift_mul();
@@ -679,12 +734,17 @@ inline void host_locator(const RecoverArgs& a, LocTable* t) {
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(kPhaseThreads) k_rec_p2(RecoverArgs a, Batch bt) {
+__global__ void __launch_bounds__(kThreads) k_rec_small(RecoverArgs a) {
+  rec_small_body<LOGN>(a, blockIdx.x);
+}
+
+template <int LOGN>
+__device__ __forceinline__ void rec_p2_body(const RecoverArgs& a, const Batch& bt, unsigned bx, int by) {
   constexpr int TL = LOGN - 4, TR = 1 << TL;
   griddep_wait();
-  const size_t w = (size_t)blockIdx.x * kPhaseThreads + threadIdx.x;
+  const size_t w = (size_t)bx * kPhaseThreads + threadIdx.x;
   if (w >= bt.ncw) return;
-  const int b = blockIdx.y;
+  const int b = by;
   uint32_t y[TR][8];
 #pragma unroll
   for (int m = 0; m < TR; m++) xload(bt.s1, bt.ncw, b + 16 * m, w, y[m]);
@@ -694,6 +754,10 @@ __global__ void __launch_bounds__(kPhaseThreads) k_rec_p2(RecoverArgs a, Batch b
   griddep_trigger();
 #pragma unroll
   for (int m = 0; m < TR; m++) xstore(bt.s2, bt.ncw, b + 16 * m, w, y[m]);
+}
+template <int LOGN>
+__global__ void __launch_bounds__(kPhaseThreads) k_rec_p2(RecoverArgs a, Batch bt) {
+  rec_p2_body<LOGN>(a, bt, blockIdx.x, blockIdx.y);
 }
 
 // blockIdx.y indexes the list of groups holding at least one erasure.
@@ -705,13 +769,13 @@ struct GroupList {
 
 // R1 (split): lambda-scale + bottom IFFT of group g = blockIdx.y.
 template <int LOGN>
-__global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
+__device__ __forceinline__ void rec_b1_body(const RecoverArgs& a, const Batch& bt, unsigned bx, int by, uint32_t* st,
+                                            const LocTable& loc) {
   constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int G = (1 << LOGN) / 16;
-  extern __shared__ uint32_t st[];
-  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw, bx);
   const ShiftMul km = make_shift_mul();
-  const int g = blockIdx.y;
+  const int g = by;
   const int row0 = 16 * g + RW * q.q;
   uint32_t x[RW][8];
   zero_rows(x);
@@ -758,15 +822,13 @@ __global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch b
 // registers, plus, for each cross-warp bit j that is clear in the warp's rows,
 // the ORIGINAL row i of the warp whose rows have bit j set.
 template <int LOGN>
-__global__ void __launch_bounds__(kSplitThreads)
-    k_rec_b3(RecoverArgs a, Batch bt, GroupList gl, const __grid_constant__ LocTable loc) {
+__device__ __forceinline__ void rec_b3_body(const RecoverArgs& a, const Batch& bt, unsigned bx, int g, uint32_t* st,
+                                            const LocTable& loc) {
   griddep_wait();
   constexpr int RW = kRowsPerWarp, WG = Split<RW>::WG, LR = Split<RW>::LR;
   constexpr int G = (1 << LOGN) / 16;
-  extern __shared__ uint32_t st[];
-  const SplitPos<RW> q = split_pos<RW>(bt.ncw);
+  const SplitPos<RW> q = split_pos<RW>(bt.ncw, bx);
   const ShiftMul km = make_shift_mul();
-  const int g = gl.g[blockIdx.y];
   const int row0 = 16 * g + RW * q.q;
   const int tid = threadIdx.x;
   uint32_t x[RW][8];
@@ -832,6 +894,69 @@ __global__ void __launch_bounds__(kSplitThreads)
       gstore(a.rx, r, row_pitch(a), a.L, bt.cw0 + q.w, y, km);
     }
   }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
+  extern __shared__ uint32_t st[];
+  rec_b1_body<LOGN>(a, bt, blockIdx.x, blockIdx.y, st, loc);
+}
+template <int LOGN>
+__global__ void __launch_bounds__(kSplitThreads)
+    k_rec_b3(RecoverArgs a, Batch bt, GroupList gl, const __grid_constant__ LocTable loc) {
+  extern __shared__ uint32_t st[];
+  rec_b3_body<LOGN>(a, bt, blockIdx.x, gl.g[blockIdx.y], st, loc);
+}
+
+// Grouped recover (see EncJob): gmask bit g is set when row group g holds an
+// erasure of this codeword; the last pass runs only those groups.
+struct RecJob {
+  RecoverArgs a;
+  uint32_t* s1;
+  uint32_t* s2;
+  size_t ncw;
+  uint32_t gmask;
+  LocTable loc;
+};
+// Grouped n <= 16 recover (the whole column in registers, own locator).
+template <int LOGN>
+__global__ void __launch_bounds__(kThreads) k_rec_small_jobs(const RecJob* __restrict__ jobs) {
+  const RecJob& j = jobs[blockIdx.z];
+  if ((size_t)blockIdx.x * (kThreads / 32) * 1024 >= j.a.L) return;
+  rec_small_body<LOGN>(j.a, blockIdx.x);
+}
+
+// The erasure tables of every codeword of a group, one warp per codeword
+// (the same log-domain tables host_locator computes for a single call).
+static __global__ void __launch_bounds__(32) k_rec_jobs_locator(RecJob* __restrict__ jobs) {
+  __shared__ uint8_t s_er[256], s_lam[256], s_ilp[256];
+  RecJob& j = jobs[blockIdx.x];
+  erasure_locator_warp(j.a, c_tab, s_er, s_lam, s_ilp);
+  __syncwarp();
+  for (int i = threadIdx.x; i < j.a.n; i += 32) {
+    j.loc.er[i] = s_er[i];
+    j.loc.lam[i] = s_lam[i];
+    j.loc.ilp[i] = s_ilp[i];
+  }
+}
+template <int LOGN>
+__global__ void __launch_bounds__(kSplitThreads) k_rec_b1_jobs(const RecJob* __restrict__ jobs) {
+  extern __shared__ uint32_t st[];
+  const RecJob& j = jobs[blockIdx.z];
+  if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw) return;
+  rec_b1_body<LOGN>(j.a, Batch{j.s1, j.s2, j.ncw, 0}, blockIdx.x, blockIdx.y, st, j.loc);
+}
+template <int LOGN>
+__global__ void __launch_bounds__(kPhaseThreads) k_rec_p2_jobs(const RecJob* __restrict__ jobs) {
+  const RecJob& j = jobs[blockIdx.z];
+  rec_p2_body<LOGN>(j.a, Batch{j.s1, j.s2, j.ncw, 0}, blockIdx.x, blockIdx.y);
+}
+template <int LOGN>
+__global__ void __launch_bounds__(kSplitThreads) k_rec_b3_jobs(const RecJob* __restrict__ jobs) {
+  extern __shared__ uint32_t st[];
+  const RecJob& j = jobs[blockIdx.z];
+  if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw || !((j.gmask >> blockIdx.y) & 1u)) return;
+  rec_b3_body<LOGN>(j.a, Batch{j.s1, j.s2, j.ncw, 0}, blockIdx.x, blockIdx.y, st, j.loc);
 }
 
 // ---- launchers ------------------------------------------------------------
@@ -942,6 +1067,74 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
   }
 }
 
+// Grouped launches: `count` codewords of one shape, descriptors in device
+// memory; max_ncw = the largest codeword's colwords.
+template <int LOGN, int LOGT>
+cudaError_t launch_enc_jobs(const EncJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  if constexpr (LOGT <= 4) {
+    constexpr size_t smem = (LOGT == 4) ? (size_t)8 * 16 * 8 * 32 * 4 : 0;
+    if (smem) {
+      cudaError_t e = cudaFuncSetAttribute(k_enc_small_jobs<LOGN, LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    const size_t slices = (max_ncw + 31) / 32;
+    for (int j0 = 0; j0 < count; j0 += 65535) {
+      const unsigned cnt = (unsigned)(count - j0 < 65535 ? count - j0 : 65535);
+      k_enc_small_jobs<LOGN, LOGT><<<dim3((unsigned)((slices + 7) / 8), 1, cnt), kThreads, smem, s>>>(d + j0);
+      count_launches(1);
+    }
+    return cudaGetLastError();
+  } else {
+    constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
+    constexpr int SCW = Split<kRowsPerWarp>::CW;
+    constexpr size_t kStage = Split<kRowsPerWarp>::kStage;
+    const unsigned gs = (unsigned)((max_ncw + SCW - 1) / SCW);
+    const unsigned gx = (unsigned)((max_ncw + kPhaseThreads - 1) / kPhaseThreads);
+    for (int j0 = 0; j0 < count; j0 += 65535) {
+      const unsigned cnt = (unsigned)(count - j0 < 65535 ? count - j0 : 65535);
+      k_enc_b1_jobs<LOGN, LOGT><<<dim3(gs, C * G, cnt), kSplitThreads, kStage, s>>>(d + j0);
+      cudaError_t e = launch_dependent(k_enc_p2_jobs<LOGN, LOGT>, dim3(gx, 16, cnt), dim3(kPhaseThreads), 0, s,
+                                       d + j0);
+      if (e == cudaSuccess)
+        e = launch_dependent(k_enc_b3_jobs<LOGN, LOGT>, dim3(gs, G, cnt), dim3(kSplitThreads), kStage, s, d + j0);
+      if (e != cudaSuccess) return e;
+      count_launches(3);
+    }
+    return cudaGetLastError();
+  }
+}
+
+template <int LOGN>
+cudaError_t launch_rec_jobs(RecJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  if constexpr (LOGN <= 4) {
+    const size_t slices = (max_ncw + 31) / 32;
+    for (int j0 = 0; j0 < count; j0 += 65535) {
+      const unsigned cnt = (unsigned)(count - j0 < 65535 ? count - j0 : 65535);
+      k_rec_small_jobs<LOGN><<<dim3((unsigned)((slices + 7) / 8), 1, cnt), kThreads, 0, s>>>(d + j0);
+      count_launches(1);
+    }
+    return cudaGetLastError();
+  } else {
+    constexpr int G = (1 << LOGN) / 16;
+    constexpr int SCW = Split<kRowsPerWarp>::CW;
+    constexpr size_t kStage = Split<kRowsPerWarp>::kStage;
+    const unsigned gs = (unsigned)((max_ncw + SCW - 1) / SCW);
+    const unsigned gx = (unsigned)((max_ncw + kPhaseThreads - 1) / kPhaseThreads);
+    for (int j0 = 0; j0 < count; j0 += 65535) {
+      const unsigned cnt = (unsigned)(count - j0 < 65535 ? count - j0 : 65535);
+      k_rec_jobs_locator<<<cnt, 32, 0, s>>>(d + j0);
+      k_rec_b1_jobs<LOGN><<<dim3(gs, G, cnt), kSplitThreads, kStage, s>>>(d + j0);
+      cudaError_t e = launch_dependent(k_rec_p2_jobs<LOGN>, dim3(gx, 16, cnt), dim3(kPhaseThreads), 0, s, d + j0);
+      if (e == cudaSuccess)
+        e = launch_dependent(k_rec_b3_jobs<LOGN>, dim3(gs, G, cnt), dim3(kSplitThreads), kStage, s, d + j0);
+      if (e != cudaSuccess) return e;
+      count_launches(4);
+    }
+    return cudaGetLastError();
+  }
+}
+
 // Scratch bytes a call needs for one batch covering the whole shard
 // (callers may provide less: the launchers then batch the columns).
 inline size_t scratch_full_bytes_enc(int n, int t, size_t L) {
@@ -951,9 +1144,12 @@ inline size_t scratch_full_bytes_rec(int n, size_t L) { return n >= 32 ? (size_t
 
 // Per-shape entry points, one translation unit each (special_enc_*.cu,
 // special_rec_*.cu) so that the build parallelises.
-#define AFRS_DECLARE_ENC(LN, LT) \
-  cudaError_t launch_enc_##LN##_##LT(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s);
-#define AFRS_DECLARE_REC(LN) cudaError_t launch_rec_##LN(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s);
+#define AFRS_DECLARE_ENC(LN, LT)                                                                   \
+  cudaError_t launch_enc_##LN##_##LT(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s); \
+  cudaError_t launch_enc_jobs_##LN##_##LT(const EncJob* d, int count, size_t max_ncw, cudaStream_t s);
+#define AFRS_DECLARE_REC(LN)                                                                   \
+  cudaError_t launch_rec_##LN(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s); \
+  cudaError_t launch_rec_jobs_##LN(RecJob* d, int count, size_t max_ncw, cudaStream_t s);
 AFRS_DECLARE_ENC(1, 0)
 AFRS_DECLARE_ENC(2, 0)
 AFRS_DECLARE_ENC(2, 1)

@@ -6,5 +6,8 @@ namespace spec {
 cudaError_t launch_enc_6_2(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
   return launch_enc<6, 2>(a, sc, s);
 }
+cudaError_t launch_enc_jobs_6_2(const EncJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  return launch_enc_jobs<6, 2>(d, count, max_ncw, s);
+}
 }  // namespace spec
 }  // namespace afrs

@@ -6,5 +6,8 @@ namespace spec {
 cudaError_t launch_enc_6_4(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
   return launch_enc<6, 4>(a, sc, s);
 }
+cudaError_t launch_enc_jobs_6_4(const EncJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  return launch_enc_jobs<6, 4>(d, count, max_ncw, s);
+}
 }  // namespace spec
 }  // namespace afrs

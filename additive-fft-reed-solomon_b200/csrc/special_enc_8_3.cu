@@ -6,5 +6,8 @@ namespace spec {
 cudaError_t launch_enc_8_3(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
   return launch_enc<8, 3>(a, sc, s);
 }
+cudaError_t launch_enc_jobs_8_3(const EncJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  return launch_enc_jobs<8, 3>(d, count, max_ncw, s);
+}
 }  // namespace spec
 }  // namespace afrs

@@ -1,4 +1,6 @@
 // Dispatch of the specialised (compile-time-twiddle) kernels by shape.
+#include <cstring>
+
 #include "special.cuh"
 
 namespace afrs {
@@ -95,4 +97,126 @@ cudaError_t launch_recover_special(const RecoverArgs& a, const ScratchArena& sc,
 size_t scratch_bytes_encode(int n, int t, size_t L) { return spec::scratch_full_bytes_enc(n, t, L); }
 size_t scratch_bytes_recover(int n, size_t L) { return spec::scratch_full_bytes_rec(n, L); }
 
+
+// ---- grouped launches (afrs_batch_dev) --------------------------------------
+
+bool jobs_supported(int op, int n, int t) { return n >= 2 && n <= 256 && t >= 1 && t < n; }
+
+size_t job_desc_bytes(int op) { return op == 0 ? sizeof(spec::EncJob) : sizeof(spec::RecJob); }
+
+size_t job_scratch_bytes(int op, int n, int t, size_t L) {
+  return op == 0 ? spec::scratch_full_bytes_enc(n, t, L) : spec::scratch_full_bytes_rec(n, L);
+}
+
+size_t job_colwords(size_t L) { return spec::total_colwords(L); }
+
+void fill_enc_job(void* desc, const EncodeArgs& a, uint32_t* scratch) {
+  spec::EncJob j{};
+  j.a = a;
+  j.s1 = scratch;
+  j.ncw = spec::total_colwords(a.L);
+  std::memcpy(desc, &j, sizeof j);
+}
+
+void fill_rec_job(void* desc, const RecoverArgs& a, uint32_t* scratch) {
+  spec::RecJob j{};
+  j.a = a;
+  j.ncw = spec::total_colwords(a.L);
+  j.s1 = scratch;
+  j.s2 = scratch + (size_t)a.n * j.ncw * 8;
+  // j.loc is filled on the device (k_rec_jobs_locator) before the kernels run.
+  for (int q = 0; q < a.e; q++) j.gmask |= 1u << (a.pos[q] >> 4);
+  std::memcpy(desc, &j, sizeof j);
+}
+
+cudaError_t launch_encode_jobs(int n, int t, const void* d_jobs, int count, size_t max_ncw, cudaStream_t s) {
+  const auto* d = static_cast<const spec::EncJob*>(d_jobs);
+  const int ln = __builtin_ctz((unsigned)n), lt = __builtin_ctz((unsigned)t);
+  switch (ln) {
+    case 1:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_1_0(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    case 2:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_2_0(d, count, max_ncw, s);
+        case 1: return spec::launch_enc_jobs_2_1(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    case 3:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_3_0(d, count, max_ncw, s);
+        case 1: return spec::launch_enc_jobs_3_1(d, count, max_ncw, s);
+        case 2: return spec::launch_enc_jobs_3_2(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    case 4:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_4_0(d, count, max_ncw, s);
+        case 1: return spec::launch_enc_jobs_4_1(d, count, max_ncw, s);
+        case 2: return spec::launch_enc_jobs_4_2(d, count, max_ncw, s);
+        case 3: return spec::launch_enc_jobs_4_3(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    case 5:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_5_0(d, count, max_ncw, s);
+        case 1: return spec::launch_enc_jobs_5_1(d, count, max_ncw, s);
+        case 2: return spec::launch_enc_jobs_5_2(d, count, max_ncw, s);
+        case 3: return spec::launch_enc_jobs_5_3(d, count, max_ncw, s);
+        case 4: return spec::launch_enc_jobs_5_4(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    case 6:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_6_0(d, count, max_ncw, s);
+        case 1: return spec::launch_enc_jobs_6_1(d, count, max_ncw, s);
+        case 2: return spec::launch_enc_jobs_6_2(d, count, max_ncw, s);
+        case 3: return spec::launch_enc_jobs_6_3(d, count, max_ncw, s);
+        case 4: return spec::launch_enc_jobs_6_4(d, count, max_ncw, s);
+        case 5: return spec::launch_enc_jobs_6_5(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    case 7:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_7_0(d, count, max_ncw, s);
+        case 1: return spec::launch_enc_jobs_7_1(d, count, max_ncw, s);
+        case 2: return spec::launch_enc_jobs_7_2(d, count, max_ncw, s);
+        case 3: return spec::launch_enc_jobs_7_3(d, count, max_ncw, s);
+        case 4: return spec::launch_enc_jobs_7_4(d, count, max_ncw, s);
+        case 5: return spec::launch_enc_jobs_7_5(d, count, max_ncw, s);
+        case 6: return spec::launch_enc_jobs_7_6(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    case 8:
+      switch (lt) {
+        case 0: return spec::launch_enc_jobs_8_0(d, count, max_ncw, s);
+        case 1: return spec::launch_enc_jobs_8_1(d, count, max_ncw, s);
+        case 2: return spec::launch_enc_jobs_8_2(d, count, max_ncw, s);
+        case 3: return spec::launch_enc_jobs_8_3(d, count, max_ncw, s);
+        case 4: return spec::launch_enc_jobs_8_4(d, count, max_ncw, s);
+        case 5: return spec::launch_enc_jobs_8_5(d, count, max_ncw, s);
+        case 6: return spec::launch_enc_jobs_8_6(d, count, max_ncw, s);
+        case 7: return spec::launch_enc_jobs_8_7(d, count, max_ncw, s);
+        default: return cudaErrorNotSupported;
+      }
+    default: return cudaErrorNotSupported;
+  }
+}
+
+cudaError_t launch_recover_jobs(int n, void* d_jobs, int count, size_t max_ncw, cudaStream_t s) {
+  auto* d = static_cast<spec::RecJob*>(d_jobs);
+  switch (__builtin_ctz((unsigned)n)) {
+    case 1: return spec::launch_rec_jobs_1(d, count, max_ncw, s);
+    case 2: return spec::launch_rec_jobs_2(d, count, max_ncw, s);
+    case 3: return spec::launch_rec_jobs_3(d, count, max_ncw, s);
+    case 4: return spec::launch_rec_jobs_4(d, count, max_ncw, s);
+    case 5: return spec::launch_rec_jobs_5(d, count, max_ncw, s);
+    case 6: return spec::launch_rec_jobs_6(d, count, max_ncw, s);
+    case 7: return spec::launch_rec_jobs_7(d, count, max_ncw, s);
+    case 8: return spec::launch_rec_jobs_8(d, count, max_ncw, s);
+    default: return cudaErrorNotSupported;
+  }
+}
 }  // namespace afrs

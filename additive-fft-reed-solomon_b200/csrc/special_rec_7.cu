@@ -6,5 +6,8 @@ namespace spec {
 cudaError_t launch_rec_7(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s) {
   return launch_rec<7>(a, sc, s);
 }
+cudaError_t launch_rec_jobs_7(RecJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  return launch_rec_jobs<7>(d, count, max_ncw, s);
+}
 }  // namespace spec
 }  // namespace afrs

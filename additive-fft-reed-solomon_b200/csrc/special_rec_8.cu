@@ -6,5 +6,8 @@ namespace spec {
 cudaError_t launch_rec_8(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s) {
   return launch_rec<8>(a, sc, s);
 }
+cudaError_t launch_rec_jobs_8(RecJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  return launch_rec_jobs<8>(d, count, max_ncw, s);
+}
 }  // namespace spec
 }  // namespace afrs
