@@ -101,8 +101,9 @@ int afrs_ifft_sharded_dev(afrs_ctx* ctx, uint8_t* d_shards, size_t shard_len, ui
 int afrs_scale_dev(afrs_ctx* ctx, const uint8_t* d_src, uint8_t* d_dst, size_t len, uint8_t scalar,
                    void* stream);
 
-/* Batched path: many independent codewords of any shapes in one persistent
- * launch (no counterpart in the reference, whose methods take one codeword;
+/* Batched path: many independent codewords of any shapes in one call, run
+ * grouped by shape on the specialised kernels, the groups concurrently
+ * (no counterpart in the reference, whose methods take one codeword;
  * each job is one call of encode_systematic_sharded, rs/src/codec.rs:241-265,
  * or recover_erasure_shards, :479-569).  Device buffers.  Encode jobs write
  * parity (parity_in is treated as zero, i.e. accumulate = 0); recover jobs
