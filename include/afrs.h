@@ -112,8 +112,9 @@ int afrs_scale_dev(afrs_ctx* ctx, const uint8_t* d_src, uint8_t* d_dst, size_t l
  * 1 = queued, 0 = more erasures than t (nothing written, the reference's
  * false); < 0 = rejected (AFRS_EINVAL), nothing written.  The call returns
  * AFRS_OK once the batch is enqueued on `stream`, or < 0 when nothing was.
- * The descriptor tables live in the context; successive batches on one
- * context are ordered even across streams. */
+ * The descriptor tables and scratch live in the context, in two slots used
+ * alternately: batches on different streams may run concurrently, and a call
+ * waits on the host until the previous batch of its slot has finished. */
 #define AFRS_OP_ENCODE 0u
 #define AFRS_OP_RECOVER 1u
 typedef struct afrs_job {
