@@ -7,6 +7,7 @@
 #include <cstring>
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <tuple>
 #include <vector>
@@ -715,6 +716,8 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 // Scratch of one batch slot's grouped launches; jobs beyond it take the
 // generic persistent kernel.
 constexpr size_t kGroupScratchCap = (size_t)1 << 30;
+// Smallest shape group (sum of n * shard_len) worth its own launches.
+constexpr size_t kGroupMinBytes = (size_t)8 << 20;
 
 // A job of a batch that runs through the grouped phase kernels.
 struct GroupedJob {
@@ -732,6 +735,7 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   std::vector<int> rec;
   std::vector<uint8_t> pos;
   std::vector<GroupedJob> grouped;
+  std::vector<size_t> valid;
   size_t grp_bytes = 0;
   int max_rows = 0;
   for (size_t i = 0; i < count; i++) {
@@ -764,13 +768,25 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
       if (!j.src || !j.dst) continue;
     }
     j.status = enc ? 0 : 1;
-    // Phase-kernel shapes run grouped by shape while the slot's scratch lasts.
+    valid.push_back(i);
+  }
+  // A shape group (encode: n, t; recover: n) runs on the specialised kernels
+  // when it holds enough bytes to fill the GPU and its scratch fits the
+  // slot; the rest share one launch of the generic persistent kernel, which
+  // runs concurrently with the groups.
+  auto key = [&](const afrs_job& j) {
+    return std::make_tuple((int)j.op, (int)j.n, j.op == AFRS_OP_ENCODE ? (int)j.t : 0);
+  };
+  std::map<std::tuple<int, int, int>, size_t> group_bytes;
+  for (size_t i : valid) group_bytes[key(jobs[i])] += (size_t)jobs[i].n * jobs[i].shard_len;
+  for (size_t i : valid) {
+    const afrs_job& j = jobs[i];
+    const bool enc = j.op == AFRS_OP_ENCODE;
     const int op = enc ? 0 : 1;
-    if (afrs::jobs_supported(op, (int)j.n, (int)j.t)) {
+    if (afrs::jobs_supported(op, (int)j.n, (int)j.t) && group_bytes[key(j)] >= kGroupMinBytes) {
       const size_t need = align256(afrs::job_scratch_bytes(op, (int)j.n, (int)j.t, j.shard_len));
       if (grp_bytes + need <= kGroupScratchCap) {
-        // Recover kernels do not depend on t: one group per n.
-        grouped.push_back(GroupedJob{i, op, (int)j.n, enc ? (int)j.t : 0, grp_bytes});
+        grouped.push_back(GroupedJob{i, op, (int)j.n, std::get<2>(key(j)), grp_bytes});
         grp_bytes += need;
         continue;
       }
@@ -889,6 +905,12 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   uint8_t* d = c->batch_dev[slot];
   if ((e = cudaMemcpyAsync(d, h, upload, cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return cuda_fail(e, "batch upload");
+  // Fork the group streams right after the upload, so that the groups run
+  // concurrently with the generic kernel below.
+  const int nstreams = (int)std::min<size_t>(4, groups.size());
+  if (nstreams && (e = cudaEventRecord(c->grp_fork, s)) != cudaSuccess) return cuda_fail(e, "batch fork");
+  for (int k = 0; k < nstreams; k++)
+    if ((e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_fork, 0)) != cudaSuccess) return cuda_fail(e, "batch fork");
   if (!bj.empty()) {
     afrs::BatchLaunch bl{};
     bl.jobs = reinterpret_cast<const afrs::BatchJob*>(d + o_jobs);
@@ -909,10 +931,6 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
     return groups[x].count * groups[x].max_ncw * groups[x].n > groups[y].count * groups[y].max_ncw * groups[y].n;
   });
-  const int nstreams = (int)std::min<size_t>(4, groups.size());
-  if (nstreams && (e = cudaEventRecord(c->grp_fork, s)) != cudaSuccess) return cuda_fail(e, "batch fork");
-  for (int k = 0; k < nstreams; k++)
-    if ((e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_fork, 0)) != cudaSuccess) return cuda_fail(e, "batch fork");
   cudaError_t le = cudaSuccess;
   for (size_t q = 0; q < order.size() && le == cudaSuccess; q++) {
     const Group& gr = groups[order[q]];
