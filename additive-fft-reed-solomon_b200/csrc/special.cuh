@@ -587,12 +587,12 @@ __device__ __forceinline__ void enc_b3_body(const EncodeArgs& a, const Batch& bt
 }
 
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kSplitThreads) k_enc_b1(EncodeArgs a, Batch bt) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_enc_b1(EncodeArgs a, Batch bt) {
   extern __shared__ uint32_t st[];
   enc_b1_body<LOGN, LOGT>(a, bt, blockIdx.x, blockIdx.y, st);
 }
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kSplitThreads) k_enc_b3(EncodeArgs a, Batch bt) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_enc_b3(EncodeArgs a, Batch bt) {
   extern __shared__ uint32_t st[];
   enc_b3_body<LOGN, LOGT>(a, bt, blockIdx.x, blockIdx.y, st);
 }
@@ -606,7 +606,7 @@ struct EncJob {
   size_t ncw;
 };
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kSplitThreads) k_enc_b1_jobs(const EncJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_enc_b1_jobs(const EncJob* __restrict__ jobs) {
   extern __shared__ uint32_t st[];
   const EncJob& j = jobs[blockIdx.z];
   if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw) return;
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_enc_p2_jobs(const EncJob* __r
   enc_p2_body<LOGN, LOGT>(j.a, Batch{j.s1, nullptr, j.ncw, 0}, blockIdx.x, blockIdx.y);
 }
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kSplitThreads) k_enc_b3_jobs(const EncJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_enc_b3_jobs(const EncJob* __restrict__ jobs) {
   extern __shared__ uint32_t st[];
   const EncJob& j = jobs[blockIdx.z];
   if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw) return;
@@ -897,12 +897,12 @@ __device__ __forceinline__ void rec_b3_body(const RecoverArgs& a, const Batch& b
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(kSplitThreads) k_rec_b1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_rec_b1(RecoverArgs a, Batch bt, const __grid_constant__ LocTable loc) {
   extern __shared__ uint32_t st[];
   rec_b1_body<LOGN>(a, bt, blockIdx.x, blockIdx.y, st, loc);
 }
 template <int LOGN>
-__global__ void __launch_bounds__(kSplitThreads)
+__global__ void __launch_bounds__(kSplitThreads, 4)
     k_rec_b3(RecoverArgs a, Batch bt, GroupList gl, const __grid_constant__ LocTable loc) {
   extern __shared__ uint32_t st[];
   rec_b3_body<LOGN>(a, bt, blockIdx.x, gl.g[blockIdx.y], st, loc);
@@ -940,7 +940,7 @@ static __global__ void __launch_bounds__(32) k_rec_jobs_locator(RecJob* __restri
   }
 }
 template <int LOGN>
-__global__ void __launch_bounds__(kSplitThreads) k_rec_b1_jobs(const RecJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_rec_b1_jobs(const RecJob* __restrict__ jobs) {
   extern __shared__ uint32_t st[];
   const RecJob& j = jobs[blockIdx.z];
   if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw) return;
@@ -952,7 +952,7 @@ __global__ void __launch_bounds__(kPhaseThreads) k_rec_p2_jobs(const RecJob* __r
   rec_p2_body<LOGN>(j.a, Batch{j.s1, j.s2, j.ncw, 0}, blockIdx.x, blockIdx.y);
 }
 template <int LOGN>
-__global__ void __launch_bounds__(kSplitThreads) k_rec_b3_jobs(const RecJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_rec_b3_jobs(const RecJob* __restrict__ jobs) {
   extern __shared__ uint32_t st[];
   const RecJob& j = jobs[blockIdx.z];
   if ((size_t)blockIdx.x * Split<kRowsPerWarp>::CW >= j.ncw || !((j.gmask >> blockIdx.y) & 1u)) return;
