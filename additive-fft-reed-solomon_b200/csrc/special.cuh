@@ -13,7 +13,7 @@
 //   bottom pass (b3) of the next transform.
 // The code of a bottom pass depends on g (its twiddles do), so each CTA runs
 // one g (blockIdx.y) over many columns: every fetched instruction is used by
-// all warps of the CTA.  A bottom group is shared by a warp pair, 8 rows per
+// all warps of the CTA.  A bottom group is shared by two warps, 8 rows per
 // warp: levels 0..2 stay inside a warp and level 3 goes through shared
 // memory, which halves the registers per thread and the code per variant.
 // (A single kernel holding all rows of a column tile in shared memory runs
