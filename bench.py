@@ -224,8 +224,10 @@ def main():
     n, t, L = N_SHARDS, T_PARITY, SHARD_LEN
     k = n - t
     op_bytes = n * L
-    # 16 codewords per role: 16 * (16 MiB encode + 16 MiB recover) = 512 MiB > L2.
-    R = 16
+    # 16 codewords per role: 16 * (16 MiB encode + 16 MiB recover) = 512 MiB > L2
+    # (24 when the stream pairs do not divide 16).
+    pairs = 1 if args.serial else args.pairs
+    R = 16 if 16 % pairs == 0 else 8 * pairs
     rng = np.random.default_rng(1234 + rank)
     msg0 = oracle.random_bytes(k * L, 42 + rank)
     par0 = np.zeros(t * L, np.uint8)
@@ -249,7 +251,7 @@ def main():
     # so the steps that reuse a codeword buffer stay on one pair, in order.
     stream = torch.cuda.current_stream(dev)
     overlap = not args.serial
-    S = args.pairs if overlap else 1
+    S = pairs
     assert R % S == 0, "--pairs must divide the number of rotating codewords"
     codec_e = [afrs.Codec(n, t, device=local, context=afrs.Context(local)) for _ in range(S)]
     codec_r = [afrs.Codec(n, t, device=local, context=afrs.Context(local)) for _ in range(S)]
@@ -447,7 +449,7 @@ def main():
                    "overlap": (f"encode and recover of a step on two streams; steps round-robin over {S} "
                                "stream pairs (own contexts)") if overlap else "encode then recover on one stream",
                    "launch": "CUDA graph per operation and codeword, replayed" if use_graphs else "eager",
-                   "l2": f"inputs rotate over {R} encode + {R} recover codewords (512 MiB > 126 MB L2)"},
+                   "l2": f"inputs rotate over {R} encode + {R} recover codewords ({R * 2 * op_bytes >> 20} MiB > 126 MB L2)"},
         "encode_gbs": round(op_bytes / (enc_iso * 1e-3) / 1e9, 2),
         "recover_gbs": round(op_bytes / (rec_iso * 1e-3) / 1e9, 2),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
