@@ -410,3 +410,40 @@ def test_host_registered_buffers(afrs):
     sub[:] = _erase(cw, L, pos)
     assert afrs.Codec(n, t).recover_erasure_shards(sub, None, L, pos)
     assert (sub == cw).all()
+
+
+@pytest.mark.gpu
+def test_batch_large_shape_groups_match_oracle(afrs):
+    """Shape groups of at least 8 MiB run on the grouped specialised kernels
+    (codeword per blockIdx.z): phase shapes, t <= 16 encodes, n <= 16
+    recovers, ragged shard lengths, one recover group holding several t;
+    small groups alongside take the generic kernel.  Byte-exact results."""
+    rng = np.random.default_rng(2024)
+    specs = [(0, 256, 128, 3000, 12), (1, 256, 128, 3000, 12), (1, 256, 32, 2100, 16), (0, 64, 8, 4096, 33),
+             (0, 128, 16, 2048, 33), (0, 64, 32, 4099, 33), (1, 16, 4, 16384, 33), (1, 128, 64, 2048, 33),
+             (0, 32, 8, 100, 5), (1, 64, 16, 77, 5)]
+    jobs, expect = [], []
+    for q, (op, n, t, L, count) in enumerate(specs):
+        for i in range(count):
+            msg = oracle.random_bytes((n - t) * L, 7000 + 97 * q + i)
+            par = np.zeros(t * L, np.uint8)
+            oracle.encode_systematic_sharded(n, t, msg, par, L)
+            if op == 0:
+                d_par = torch.full((t * L,), 0x3C, dtype=torch.uint8, device="cuda")
+                jobs.append(afrs.Job.encode(n, t, torch.from_numpy(msg).cuda(), d_par, L))
+                expect.append(par)
+            else:
+                cw = np.concatenate([par, msg])
+                pos = rng.choice(n, int(rng.integers(1, t + 1)), replace=False).tolist()
+                rx = cw.copy()
+                for p in pos:
+                    rx[p * L:(p + 1) * L] = 0xC3
+                jobs.append(afrs.Job.recover(n, t, torch.from_numpy(rx).cuda(), L, pos))
+                expect.append(cw)
+    launches0 = afrs.lib().afrs_kernel_launches()
+    status = afrs.run_batch(jobs)
+    torch.cuda.synchronize()
+    assert afrs.lib().afrs_kernel_launches() - launches0 > 2  # grouped launches, not only the generic kernel
+    for j, ex, st in zip(jobs, expect, status):
+        assert st == (0 if j.op == 0 else 1)
+        assert (j.dst.cpu().numpy() == ex).all(), (j.op, j.n, j.t, j.shard_len)
