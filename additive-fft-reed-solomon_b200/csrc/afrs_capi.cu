@@ -814,8 +814,8 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   }
   if (tasks.size() > (size_t)INT32_MAX) return fail(AFRS_EINVAL, "too many tiles");
   if (bj.empty() && grouped.empty()) return AFRS_OK;
-  // Groups of one shape, in order of first appearance; descriptors of a
-  // group form one array.
+  // Jobs sorted by shape (stable: caller order within a shape); the
+  // descriptors of one shape group form one array.
   std::stable_sort(grouped.begin(), grouped.end(), [](const GroupedJob& x, const GroupedJob& y) {
     return std::make_tuple(x.op, x.n, x.t) < std::make_tuple(y.op, y.n, y.t);
   });
