@@ -48,3 +48,18 @@ def test_no_device_context_fails_cleanly(afrs):
     h = ctypes.c_void_p()
     r = afrs.lib().afrs_ctx_create(0, ctypes.byref(h))
     assert r < 0 and not h.value
+
+
+def test_newer_entry_points_validate_arguments(afrs):
+    """No device needed: invalid arguments are rejected before any CUDA call."""
+    import ctypes
+
+    lib = afrs.lib()
+    E = afrs._lib.AFRS_EINVAL
+    assert lib.afrs_ctx_set_staging(None, 0, 0, 0) == E
+    assert lib.afrs_syndrome_dev(None, 4, 2, None, 16, None, None, None) == E
+    assert lib.afrs_batch_dev(None, None, 0, None) == E
+    a, b = ctypes.c_uint64(7), ctypes.c_uint64(7)
+    lib.afrs_staged_bytes(ctypes.byref(a), ctypes.byref(b))
+    assert a.value >= 0 and b.value >= 0
+    lib.afrs_staged_bytes(None, None)  # either pointer may be NULL
