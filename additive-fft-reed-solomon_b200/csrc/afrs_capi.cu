@@ -106,7 +106,7 @@ cudaError_t ensure_scratch(afrs_ctx* c, size_t bytes) {
 }
 
 // Largest phase scratch a context keeps (the launchers batch columns beyond it).
-constexpr size_t kWorkCap = (size_t)128 << 20;
+constexpr size_t kWorkCap = (size_t)1 << 30;
 
 // Grows the context's phase scratch to min(need, kWorkCap) and orders this
 // call after the previous user of the scratch (calls on different streams

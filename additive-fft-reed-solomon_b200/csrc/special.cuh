@@ -19,8 +19,9 @@
 // (A single kernel holding all rows of a column tile in shared memory runs
 // each variant once per tile and is bound by instruction fetch: ~800 KB of
 // straight-line code for n = 256.)
-// Between phases the rows stay bit-sliced in a scratch buffer (128 MiB at
-// most, largely L2-resident); long shards are processed in column batches.
+// Between phases the rows stay bit-sliced in a scratch buffer (1 GiB at most;
+// L2-resident for small codewords); longer shards are processed in column
+// batches.
 // Transforms with k <= 4 run entirely inside one thread.
 #pragma once
 #include <utility>
@@ -980,8 +981,11 @@ cudaError_t launch_dependent(void (*k)(KArgs...), dim3 grid, dim3 block, size_t 
   return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
 }
 
-// Scratch budget per phase batch: both buffers together stay well inside L2.
-constexpr size_t kScratchBudget = (size_t)128 << 20;
+// Scratch budget per column batch.  Larger batches mean fewer launches and
+// fuller waves, which outweighs keeping the scratch inside L2: n = 256 with
+// 4 MiB shards, recover 1856 us (128 MiB) -> 1623 (256) -> 1463 (512) ->
+// 1407 us (1 GiB).
+constexpr size_t kScratchBudget = (size_t)1 << 30;
 
 // Colwords covering L bytes in the io.cuh layout (whole 1024-column slices).
 inline size_t total_colwords(size_t L) { return (L + 1023) / 1024 * 32; }

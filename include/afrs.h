@@ -67,7 +67,7 @@ int afrs_recover(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* received, size_
  * (a cudaStream_t; NULL = the legacy default stream).  Positions are read
  * from host memory during the call.  For t >= 32 (encode) and n >= 32
  * (recover) the kernels keep intermediate rows in a device scratch buffer
- * owned by the context: the first call of a size grows it (at most 128 MiB;
+ * owned by the context: the first call of a size grows it (at most 1 GiB;
  * longer shards are processed in column batches), and calls that share a
  * context are ordered on that buffer even when they use different streams. */
 int afrs_encode_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, const uint8_t* d_message,
