@@ -117,16 +117,30 @@ class ClockSampler:
                 "in_timed_region": bool(inside)}
 
 
+_PER_PAIR = None
+
+
+def cpu_per_pair() -> float:
+    """Seconds for one encode + one recover on one host thread (probed once)."""
+    global _PER_PAIR
+    if _PER_PAIR is None:
+        from oracle import oracle
+
+        n, t, L = N_SHARDS, T_PARITY, SHARD_LEN
+        probe_e = oracle.gfni_throughput("encode", n, t, L, 1, 1)
+        probe_r = oracle.gfni_throughput("recover", n, t, L, 1, 1)
+        _PER_PAIR = n * L / probe_e + n * L / probe_r
+    return _PER_PAIR
+
+
 def cpu_baseline(seconds: float, threads: int):
     """GFNI restatement of the reference's kernel + codec on host cores, on a
-    bounded sample of the same workload (same n, t, L)."""
+    bounded sample of the same workload (same n, t, L): about `seconds` of
+    work, at least one encode and one recover per thread."""
     from oracle import oracle
 
     n, t, L = N_SHARDS, T_PARITY, SHARD_LEN
-    probe_e = oracle.gfni_throughput("encode", n, t, L, 1, 1)
-    probe_r = oracle.gfni_throughput("recover", n, t, L, 1, 1)
-    per_pair = n * L / probe_e + n * L / probe_r  # seconds for one encode + one recover, one thread
-    iters = max(1, int(seconds / max(per_pair, 1e-6) / 2))
+    iters = max(1, int(seconds / max(cpu_per_pair(), 1e-6) / 2))
     enc = oracle.gfni_throughput("encode", n, t, L, iters, threads, 42)
     rec = oracle.gfni_throughput("recover", n, t, L, iters, threads, 43)
     combined = 2.0 / (1.0 / enc + 1.0 / rec)  # same mix as one GPU step: one encode + one recover
@@ -160,17 +174,25 @@ def run_reference(args):
     vals = []
     enc = rec = 0.0
     sample = ""
-    for _ in range(args.warmup):
-        cpu_baseline(0.5, threads)
+    # Each step is a sample of about min(2 s, 90 s / steps) of CPU work (at
+    # least one encode + one recover per thread); samples are taken until
+    # `steps` are done or 90 s of wall time have passed (at least 3), so the
+    # run stays within a few minutes for any --steps.
+    per_step = min(2.0, 90.0 / max(1, args.steps))
+    for _ in range(min(args.warmup, 3)):
+        cpu_baseline(per_step, threads)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, enc, rec, sample = cpu_baseline(2.0, threads)
+    samples = 0
+    while samples < args.steps and (samples < 3 or time.perf_counter() - t0 < 90.0):
+        v, enc, rec, sample = cpu_baseline(per_step, threads)
         vals.append(v)
+        samples += 1
     wall = time.perf_counter() - t0
+    sample = f"{samples} samples of {sample}"
     value = statistics.median(vals)
     out = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * wall / max(args.steps, 1), 3),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * wall / samples, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": N_SHARDS, "k": N_SHARDS - T_PARITY, "t": T_PARITY,
                    "shard_len": SHARD_LEN, "erasures": T_PARITY},
