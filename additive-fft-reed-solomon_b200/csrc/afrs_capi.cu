@@ -82,11 +82,15 @@ int check_positions(uint32_t n, const uint8_t* pos, size_t e) {
   return AFRS_OK;
 }
 
+// Makes `dev` current for the call.  cudaSetDevice runs even when `dev` is
+// already the thread's device: in a host thread that has made no CUDA call
+// yet it binds the device's context, without which cudaPointerGetAttributes
+// reports page-locked memory without its device address.
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
     cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
+    cudaSetDevice(dev);
   }
   ~DeviceGuard() {
     int cur = -1;

@@ -386,6 +386,32 @@ def test_direct_path_for_page_locked_buffers(afrs, n, t, L):
 
 
 @pytest.mark.gpu
+def test_direct_path_from_a_fresh_host_thread(afrs):
+    """The first call of a host thread that has made no CUDA call yet still
+    takes the direct path: exactly the surviving shards in, the erased out."""
+    import threading
+
+    n, t, L = 256, 128, 65536
+    msg, par = _codeword(n, t, L, seed=5)
+    cw = np.concatenate([par, msg])
+    pos = sorted(np.random.default_rng(9).choice(n, t, replace=False).tolist())
+    h_rx = _pinned(_erase(cw, L, pos))
+    codec = afrs.Codec(n, t)
+    out = {}
+
+    def run():
+        b0 = _staged_bytes(afrs)
+        out["ok"] = codec.recover_erasure_shards(h_rx, None, L, pos)
+        out["moved"] = tuple(b - a for a, b in zip(b0, _staged_bytes(afrs)))
+
+    th = threading.Thread(target=run)
+    th.start()
+    th.join()
+    assert out["ok"] and (h_rx == cw).all()
+    assert out["moved"] == ((n - t) * L, t * L)
+
+
+@pytest.mark.gpu
 def test_host_registered_buffers(afrs):
     """Memory page-locked with cudaHostRegister (whose device alias may differ
     from its host address) and a sub-range of a page-locked buffer."""
