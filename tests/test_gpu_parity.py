@@ -412,6 +412,43 @@ def test_direct_path_from_a_fresh_host_thread(afrs):
 
 
 @pytest.mark.gpu
+def test_host_api_from_concurrent_threads(afrs):
+    """Pairs of host threads (one encoding, one recovering, own contexts and
+    buffers) running back to back at once give the oracle's results."""
+    import threading
+
+    n, t, L, P, steps = 64, 16, 4096, 3, 6
+    msg, par = _codeword(n, t, L, seed=41)
+    cw = np.concatenate([par, msg])
+    pos = sorted(np.random.default_rng(4).choice(n, t, replace=False).tolist())
+    h_msg = _pinned(msg)
+    pars = [_pinned(np.zeros(t * L, np.uint8)) for _ in range(P)]
+    rxs = [_pinned(_erase(cw, L, pos)) for _ in range(P)]
+    encs = [afrs.Codec(n, t, context=afrs.Context(0)) for _ in range(P)]
+    recs = [afrs.Codec(n, t, context=afrs.Context(0)) for _ in range(P)]
+    errors = []
+
+    def work(i, enc):
+        try:
+            for _ in range(steps):
+                if enc:
+                    encs[i].encode_parity(h_msg, pars[i], L)
+                else:
+                    assert recs[i].recover_erasure_shards(rxs[i], None, L, pos)
+        except Exception as ex:  # surfaced below
+            errors.append(ex)
+
+    ths = [threading.Thread(target=work, args=(i, e)) for i in range(P) for e in (True, False)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    assert not errors
+    for i in range(P):
+        assert (pars[i] == par).all() and (rxs[i] == cw).all()
+
+
+@pytest.mark.gpu
 def test_host_registered_buffers(afrs):
     """Memory page-locked with cudaHostRegister (whose device alias may differ
     from its host address) and a sub-range of a page-locked buffer."""
