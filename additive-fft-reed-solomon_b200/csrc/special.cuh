@@ -24,6 +24,8 @@
 // batches.
 // Transforms with k <= 4 run entirely inside one thread.
 #pragma once
+#include <array>
+#include <cstring>
 #include <utility>
 
 #include "afrs_internal.h"
@@ -702,36 +704,71 @@ inline int host_mod255(int v) {
   return v < 0 ? v + 255 : v;
 }
 
-inline void host_fwht255(int* v, int n) {
+// Integer Walsh-Hadamard transform, no reduction: the transform is linear
+// over the integers, so reducing mod 255 once at the end equals reducing at
+// every step.  |inputs| <= 64516 (254 * 254) and n <= 256 keep every value
+// within 32 bits.
+inline void host_fwht(int* v, int n) {
   for (int h = 1; h < n; h <<= 1)
     for (int i = 0; i < n; i += 2 * h)
       for (int j = i; j < i + h; j++) {
         const int x = v[j], y = v[j + h];
-        v[j] = host_mod255(x + y);
-        v[j + h] = host_mod255(x - y);
+        v[j] = x + y;
+        v[j + h] = x - y;
       }
+}
+
+// Transform of log(omega_x) (0 at x = 0) mod 255 for n = 2^k points; it
+// depends on n only, so it is computed once per n.
+inline const int* host_log_omega_wht(int n) {
+  static const std::array<std::array<int, 256>, 9> tabs = [] {
+    std::array<std::array<int, 256>, 9> t{};
+    for (int k = 0; k <= 8; k++) {
+      const int m = 1 << k;
+      int v[256] = {};
+      for (int x = 1; x < m; x++) v[x] = kField.log[kField.omega[x]];
+      host_fwht(v, m);
+      for (int x = 0; x < m; x++) t[k][x] = host_mod255(v[x]);
+    }
+    return t;
+  }();
+  return tabs[__builtin_ctz((unsigned)n)].data();
 }
 
 inline void host_locator(const RecoverArgs& a, LocTable* t) {
   const int n = a.n;
-  int ve[256] = {}, vl[256] = {};
+  int ve[256] = {};
   *t = LocTable{};
-  for (int j = 0; j < a.e; j++) t->er[a.pos[j]] = 1;
-  for (int x = 0; x < n; x++) {
-    ve[x] = t->er[x];
-    vl[x] = x ? kField.log[kField.omega[x]] : 0;
+  for (int j = 0; j < a.e; j++) {
+    t->er[a.pos[j]] = 1;
+    ve[a.pos[j]] = 1;
   }
-  host_fwht255(ve, n);
-  host_fwht255(vl, n);
-  for (int x = 0; x < n; x++) ve[x] = host_mod255(ve[x] * vl[x]);
-  host_fwht255(ve, n);
+  host_fwht(ve, n);
+  const int* wl = host_log_omega_wht(n);
+  for (int x = 0; x < n; x++) ve[x] = host_mod255(ve[x]) * wl[x];
+  host_fwht(ve, n);
   const int k = __builtin_ctz((unsigned)n);
   const int ninv = (1 << (8 - k)) % 255;
   for (int x = 0; x < n; x++) {
-    const int sv = host_mod255(ve[x] * ninv);
+    const int sv = host_mod255(host_mod255(ve[x]) * ninv);
     t->lam[x] = (uint8_t)sv;
     t->ilp[x] = (uint8_t)host_mod255(255 - sv);
   }
+}
+
+// The column windows and batches of one call, and repeated calls with one
+// erasure pattern, share a locator: each host thread keeps its last one.
+inline const LocTable& cached_locator(const RecoverArgs& a) {
+  thread_local LocTable t;
+  thread_local int n = 0, e = -1;
+  thread_local uint8_t pos[256];
+  if (a.n != n || a.e != e || std::memcmp(pos, a.pos, (size_t)a.e) != 0) {
+    host_locator(a, &t);
+    n = a.n;
+    e = a.e;
+    std::memcpy(pos, a.pos, (size_t)a.e);
+  }
+  return t;
 }
 
 template <int LOGN>
@@ -1048,8 +1085,7 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
     for (int g = 0; g < G; g++)
       if (has[g]) gl.g[gl.count++] = (uint8_t)g;
     const size_t total_cw = total_colwords(a.L);
-    LocTable loc;
-    host_locator(a, &loc);
+    const LocTable& loc = cached_locator(a);
     const size_t bcw = batch_colwords(N, 2, sc.bytes, total_cw);
     if (bcw == 0) return cudaErrorMemoryAllocation;
 
