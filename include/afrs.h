@@ -65,9 +65,10 @@ int afrs_recover(afrs_ctx* ctx, uint32_t n, uint32_t t, uint8_t* received, size_
 
 /* Device-pointer variants of the two calls above, enqueued on `stream`
  * (a cudaStream_t; NULL = the legacy default stream).  Positions are read
- * from host memory during the call.  For t >= 32 (encode) and n >= 32
- * (recover) the kernels keep intermediate rows in a device scratch buffer
- * owned by the context: the first call of a size grows it (at most 1 GiB;
+ * from host memory during the call.  Encodes with t >= 32 and recovers with
+ * n >= 32 keep intermediate rows in a device scratch buffer owned by the
+ * context (except encodes with n <= 64 of at most 4 MiB per codeword, which
+ * run as one launch without it): the first call of a size grows it (at most 1 GiB;
  * longer shards are processed in column batches), and calls that share a
  * context are ordered on that buffer even when they use different streams. */
 int afrs_encode_dev(afrs_ctx* ctx, uint32_t n, uint32_t t, const uint8_t* d_message,
