@@ -154,18 +154,16 @@ cudaError_t release_work(afrs_ctx* c, cudaStream_t s) {
 
 // Shapes where the one-launch generic kernel is faster per call than the
 // specialised ones (measured on a B200, codewords up to 4 MiB): encodes with
-// 16 < n and t <= 16, whose specialised kernel runs a codeword's chunks one
-// after another in one warp per 1024 columns (n = 256, t = 16, 1 KiB shards:
-// 137 vs 33 us; n = 32, t = 16, 64 KiB: 27 vs 8 us; n = 256, t = 4, 16 KiB:
-// 105 vs 76 us), and encodes with n <= 64, where three phase launches cost
-// more than the work (n = 64, t = 32, 1 KiB: 13.9 vs 8.2 us).  Beyond 4 MiB
-// the generic kernel's time grows with the bytes and the specialised ones
-// win (n = 32, t = 16, 1 MiB shards: 68 vs 28 us).  The generic kernel takes
-// compact rows (no row pitch).
+// t = 16 and n >= 32 (n = 32, 1 KiB shards: 6.2 vs 27.6 us; n = 64: 10 vs
+// 26.5 us; n = 256: 33 vs 44 us), and encodes with t >= 32 and n <= 64, where
+// three phase launches cost more than the work (n = 64, t = 32, 1 KiB: 8.2
+// vs 13.9 us).  Beyond 4 MiB the generic kernel's time grows with the bytes
+// and the specialised ones win (n = 32, t = 16, 1 MiB shards: 68 vs 28 us).
+// The generic kernel takes compact rows (no row pitch).
 bool generic_encode_wins(const afrs::EncodeArgs& a) {
   if (a.pitch && a.pitch != a.L) return false;
   if ((size_t)a.n * a.L > ((size_t)4 << 20)) return false;
-  return a.t <= 16 ? a.n >= 32 : a.n <= 64;
+  return a.t <= 16 ? a.t == 16 && a.n >= 32 : a.n <= 64;
 }
 
 int launch_encode(afrs_ctx* c, const afrs::EncodeArgs& a, cudaStream_t s) {

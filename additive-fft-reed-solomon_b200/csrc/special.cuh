@@ -184,9 +184,107 @@ __device__ __forceinline__ void zero_rows(uint32_t (&x)[NR][8]) {
 // ---- encode, t <= 16: one warp per 1024-column slice ----------------------
 // codec.rs:241-265: parity = FFT_t(parity_in? ^ sum_c IFFT_t(chunk c, omega_ct), 0),
 // chunk c = message shards (c-1)t .. ct-1, c = 1 .. n/t - 1.
+// t <= 16 with more than one chunk: the CTA's warps share one 1024-column
+// slice and split its chunks (warp w takes chunks w + 1, w + 1 + W, ...),
+// each XOR-accumulating its chunk IFFTs in its own shared-memory rows; the
+// rows are then summed over the warps and warp 0 runs the final FFT.  (One
+// warp running all n/t - 1 chunks of a slice made the time of a small
+// codeword the serial latency of its chunks.)
 template <int LOGN, int LOGT>
+__device__ __forceinline__ void enc_small_split_body(const EncodeArgs& a, unsigned bx, uint32_t* sm) {
+  constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, W = kThreads / 32;
+  constexpr int WU = C < W ? C : W;  // warps that get chunks
+  constexpr int kRows = T * 8 * 32;  // words of one warp's accumulator
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if ((size_t)bx * 1024 >= a.L) return;  // the whole CTA
+  const size_t cw = (size_t)bx * 32 + lane;
+  const ShiftMul km = make_shift_mul();
+  if (warp < WU) {
+    uint32_t* wacc = sm + warp * kRows;
+    for (int c = 1 + warp; c <= C; c += W) {
+      uint32_t x[T][8];
+#pragma unroll
+      for (int r = 0; r < T; r++) gload(a.msg, (size_t)(c - 1) * T + r, row_pitch(a), a.L, cw, x[r], km);
+      if constexpr (LOGT > 0) {
+        dispatch<1, C>(c, [&](auto cc) {
+          constexpr int CC = decltype(cc)::value;
+          block_ifft<0, LOGT, 0, omega_c(CC * T), T>(x);
+        });
+      }
+      const bool first = c == 1 + warp;
+#pragma unroll
+      for (int r = 0; r < T; r++) {
+        uint32_t y[8];
+        if (first) {
+#pragma unroll
+          for (int p = 0; p < 8; p++) y[p] = x[r][p];
+        } else {
+          sload<32>(wacc, r, lane, y);
+#pragma unroll
+          for (int p = 0; p < 8; p++) y[p] ^= x[r][p];
+        }
+        sstore<32>(wacc, r, lane, y);
+      }
+    }
+  }
+  __syncthreads();
+  for (int r = warp; r < T; r += W) {
+    uint32_t y[8];
+    sload<32>(sm, r, lane, y);
+    for (int w = 1; w < WU; w++) {
+      uint32_t z[8];
+      sload<32>(sm + w * kRows, r, lane, z);
+#pragma unroll
+      for (int p = 0; p < 8; p++) y[p] ^= z[p];
+    }
+    sstore<32>(sm, r, lane, y);
+  }
+  __syncthreads();
+  if (warp != 0) return;
+  uint32_t f[T][8];
+#pragma unroll
+  for (int r = 0; r < T; r++) {
+    sload<32>(sm, r, lane, f[r]);
+    if (a.accumulate) {
+      uint32_t y[8];
+      gload(a.parity, r, row_pitch(a), a.L, cw, y, km);
+#pragma unroll
+      for (int p = 0; p < 8; p++) f[r][p] ^= y[p];
+    }
+  }
+  block_fft<0, LOGT, 0, 0, T>(f);
+#pragma unroll
+  for (int r = 0; r < T; r++) gstore(a.parity, r, row_pitch(a), a.L, cw, f[r], km);
+}
+
+// Layout of the t <= 16 encode.  With more than one chunk and few slices of
+// 1024 columns (or t < 16, where the per-warp accumulators are small), the
+// warps of a CTA split the chunks of one slice; otherwise each warp takes a
+// slice of its own and runs all its chunks (at t = 16 and long shards that is
+// faster: n = 256, 1 MiB shards: 280 vs 465 us).
+template <int LOGN, int LOGT>
+inline bool enc_small_split(size_t slices) {
+  constexpr int T = 1 << LOGT, C = ((1 << LOGN) >> LOGT) - 1;
+  return C > 1 && (T < 16 || slices <= 128);
+}
+// CTAs and dynamic shared memory of either layout.
+template <int LOGN, int LOGT>
+inline unsigned enc_small_ctas(size_t slices, bool split) {
+  return (unsigned)(split ? slices : (slices + kThreads / 32 - 1) / (kThreads / 32));
+}
+template <int LOGN, int LOGT>
+constexpr size_t enc_small_smem(bool split) {
+  constexpr int T = 1 << LOGT, C = ((1 << LOGN) >> LOGT) - 1, W = kThreads / 32;
+  return split ? (size_t)(C < W ? C : W) * T * 8 * 32 * 4 : (T == 16 ? (size_t)W * 16 * 8 * 32 * 4 : 0);
+}
+
+template <int LOGN, int LOGT, bool kSplit>
 __device__ __forceinline__ void enc_small_body(const EncodeArgs& a, unsigned bx, uint32_t* sm) {
   constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1;
+  if constexpr (kSplit && C > 1) {
+    enc_small_split_body<LOGN, LOGT>(a, bx, sm);
+    return;
+  }
   constexpr bool kSmemAcc = (T == 16);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t slice = (size_t)bx * (kThreads / 32) + warp;
@@ -295,10 +393,10 @@ __device__ __forceinline__ void cp_async16(uint4* dst, const uint8_t* src) {
 }
 
 // ---- encode, t >= 32 -------------------------------------------------------
-template <int LOGN, int LOGT>
+template <int LOGN, int LOGT, bool kSplit>
 __global__ void __launch_bounds__(kThreads) k_enc_small(EncodeArgs a) {
   extern __shared__ uint32_t sm[];
-  enc_small_body<LOGN, LOGT>(a, blockIdx.x, sm);
+  enc_small_body<LOGN, LOGT, kSplit>(a, blockIdx.x, sm);
 }
 
 // E2: top levels for rows {b + 16 m} (b = blockIdx.y): IFFT top of every
@@ -629,12 +727,12 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_enc_b3_jobs(const EncJob* 
 }
 
 // Grouped t <= 16 encode: one warp per 1024-column slice of codeword blockIdx.z.
-template <int LOGN, int LOGT>
+template <int LOGN, int LOGT, bool kSplit>
 __global__ void __launch_bounds__(kThreads) k_enc_small_jobs(const EncJob* __restrict__ jobs) {
   extern __shared__ uint32_t sm[];
   const EncJob& j = jobs[blockIdx.z];
-  if ((size_t)blockIdx.x * (kThreads / 32) * 1024 >= j.a.L) return;
-  enc_small_body<LOGN, LOGT>(j.a, blockIdx.x, sm);
+  if ((size_t)blockIdx.x * (kSplit ? 1 : kThreads / 32) * 1024 >= j.a.L) return;
+  enc_small_body<LOGN, LOGT, kSplit>(j.a, blockIdx.x, sm);
 }
 
 // ---- recover ------------------------------------------------------------
@@ -1038,14 +1136,15 @@ inline size_t batch_colwords(size_t rows_per_buffer, int buffers, size_t scratch
 template <int LOGN, int LOGT>
 cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
   if constexpr (LOGT <= 4) {
-    constexpr size_t smem = (LOGT == 4) ? (size_t)8 * 16 * 8 * 32 * 4 : 0;
-    auto fn = k_enc_small<LOGN, LOGT>;
-    if (smem) {
+    const size_t slices = (a.L + 1023) / 1024;
+    const bool split = enc_small_split<LOGN, LOGT>(slices);
+    const size_t smem = enc_small_smem<LOGN, LOGT>(split);
+    auto fn = split ? k_enc_small<LOGN, LOGT, true> : k_enc_small<LOGN, LOGT, false>;
+    if (smem > (48 << 10)) {
       cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    const size_t slices = (a.L + 1023) / 1024;
-    fn<<<(unsigned)((slices + 7) / 8), kThreads, smem, s>>>(a);
+    fn<<<enc_small_ctas<LOGN, LOGT>(slices, split), kThreads, smem, s>>>(a);
     count_launches(1);
     return cudaGetLastError();
   } else {
@@ -1112,16 +1211,17 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
 template <int LOGN, int LOGT>
 cudaError_t launch_enc_jobs(const EncJob* d, int count, size_t max_ncw, cudaStream_t s) {
   if constexpr (LOGT <= 4) {
-    constexpr size_t smem = (LOGT == 4) ? (size_t)8 * 16 * 8 * 32 * 4 : 0;
-    if (smem) {
-      cudaError_t e = cudaFuncSetAttribute(k_enc_small_jobs<LOGN, LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
+    const size_t slices = (max_ncw + 31) / 32;
+    const bool split = enc_small_split<LOGN, LOGT>(slices);
+    const size_t smem = enc_small_smem<LOGN, LOGT>(split);
+    auto fn = split ? k_enc_small_jobs<LOGN, LOGT, true> : k_enc_small_jobs<LOGN, LOGT, false>;
+    if (smem > (48 << 10)) {
+      cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    const size_t slices = (max_ncw + 31) / 32;
     for (int j0 = 0; j0 < count; j0 += 65535) {
       const unsigned cnt = (unsigned)(count - j0 < 65535 ? count - j0 : 65535);
-      k_enc_small_jobs<LOGN, LOGT><<<dim3((unsigned)((slices + 7) / 8), 1, cnt), kThreads, smem, s>>>(d + j0);
+      fn<<<dim3(enc_small_ctas<LOGN, LOGT>(slices, split), 1, cnt), kThreads, smem, s>>>(d + j0);
       count_launches(1);
     }
     return cudaGetLastError();
