@@ -39,6 +39,7 @@ SIGNATURES = {
     "afrs_version": (ctypes.c_char_p, []),
     "afrs_kernel_launches": (ctypes.c_uint64, []),
     "afrs_ctx_set_staging": (ctypes.c_int, [ctypes.c_void_p, _sz, _sz, ctypes.c_int]),
+    "afrs_ctx_set_work_cap": (ctypes.c_int, [ctypes.c_void_p, _sz]),
     "afrs_staged_bytes": (None, [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "afrs_encode": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _u8p, _sz, ctypes.c_int]),
     "afrs_recover": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, _u8p, _sz]),

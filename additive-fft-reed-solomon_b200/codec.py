@@ -63,6 +63,12 @@ class Context:
     def handle(self) -> ctypes.c_void_p:
         return self._h
 
+    def set_work_cap(self, nbytes: int) -> None:
+        """Largest device scratch the context's calls use between kernels
+        (afrs_ctx_set_work_cap); longer shards run in column batches.  0
+        restores the default."""
+        _check(_lib.lib().afrs_ctx_set_work_cap(self._h, int(nbytes)), "afrs_ctx_set_work_cap")
+
     def close(self) -> None:
         if self._h:
             _lib.lib().afrs_ctx_destroy(self._h)

@@ -22,6 +22,7 @@ struct afrs_ctx {
   size_t scratch_bytes;
   uint32_t* work;  // bit-sliced intermediate rows of the phase kernels
   size_t work_bytes;
+  size_t work_cap;  // largest phase scratch used per call (afrs_ctx_set_work_cap)
   cudaEvent_t work_free;  // recorded after each use of `work`
   // Descriptor tables of afrs_batch_dev, two slots so that one batch can be
   // prepared while the previous one runs.
@@ -111,6 +112,9 @@ cudaError_t ensure_scratch(afrs_ctx* c, size_t bytes) {
 
 // Largest phase scratch a context keeps (the launchers batch columns beyond it).
 constexpr size_t kWorkCap = (size_t)1 << 30;
+// Smallest cap afrs_ctx_set_work_cap accepts: one colword of the largest
+// recover (n = 256: two buffers of 256 rows x 32 bytes).
+constexpr size_t kMinWorkCap = (size_t)16 << 10;
 
 // Grows the context's phase scratch to min(need, kWorkCap) and orders this
 // call after the previous user of the scratch (calls on different streams
@@ -126,10 +130,11 @@ bool capturing(cudaStream_t s) {
 // dependency on work outside the graph.
 cudaError_t acquire_work(afrs_ctx* c, size_t need, cudaStream_t s, afrs::ScratchArena* out) {
   std::lock_guard<std::recursive_mutex> lk(c->mu);
-  if (need > kWorkCap) need = kWorkCap;
+  if (need > c->work_cap) need = c->work_cap;
+  const size_t usable = std::min(c->work_bytes, c->work_cap);
   if (capturing(s)) {
-    if (need > c->work_bytes) return cudaErrorStreamCaptureUnsupported;
-    *out = afrs::ScratchArena{c->work, c->work_bytes};
+    if (need > usable) return cudaErrorStreamCaptureUnsupported;
+    *out = afrs::ScratchArena{c->work, usable};
     return cudaSuccess;
   }
   if (need > c->work_bytes) {
@@ -144,7 +149,7 @@ cudaError_t acquire_work(afrs_ctx* c, size_t need, cudaStream_t s, afrs::Scratch
   }
   cudaError_t e = cudaStreamWaitEvent(s, c->work_free, 0);
   if (e != cudaSuccess) return e;
-  *out = afrs::ScratchArena{c->work, c->work_bytes};
+  *out = afrs::ScratchArena{c->work, std::min(c->work_bytes, c->work_cap)};
   return cudaSuccess;
 }
 
@@ -428,6 +433,16 @@ int afrs_ctx_set_staging(afrs_ctx* c, size_t window_bytes, size_t merge_bytes, i
   return AFRS_OK;
 }
 
+int afrs_ctx_set_work_cap(afrs_ctx* c, size_t bytes) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (bytes && bytes < kMinWorkCap)
+    return fail(AFRS_EINVAL, "work cap %zu is below the %zu-byte minimum", bytes, kMinWorkCap);
+  if (bytes > kWorkCap) return fail(AFRS_EINVAL, "work cap %zu is above the %zu-byte maximum", bytes, kWorkCap);
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->work_cap = bytes ? bytes & ~(size_t)255 : kWorkCap;
+  return AFRS_OK;
+}
+
 uint64_t afrs_kernel_launches(void) { return afrs::g_launches.load(std::memory_order_relaxed); }
 
 void afrs_staged_bytes(uint64_t* h2d, uint64_t* d2h) {
@@ -452,6 +467,7 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
   c->scratch_bytes = 0;
   c->work = nullptr;
   c->work_bytes = 0;
+  c->work_cap = kWorkCap;
   for (int i = 0; i < 2; i++) {
     c->batch_dev[i] = nullptr;
     c->batch_dev_bytes[i] = 0;
@@ -880,23 +896,29 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   DeviceGuard g(c->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // A failure before anything is enqueued leaves every accepted job unrun.
+  auto bail = [&](cudaError_t err, const char* what) -> int {
+    const int r = cuda_fail(err, what);
+    for (size_t i : valid) jobs[i].status = r;
+    return r;
+  };
   const int slot = c->batch_slot;
   c->batch_slot ^= 1;
   // The slot's previous batch must be done with its staging, tables and scratch.
   cudaError_t e = cudaEventSynchronize(c->batch_free[slot]);
-  if (e != cudaSuccess) return cuda_fail(e, "batch wait");
+  if (e != cudaSuccess) return bail(e, "batch wait");
   if (total > c->batch_dev_bytes[slot]) {
     if (c->batch_dev[slot]) cudaFree(c->batch_dev[slot]);
     c->batch_dev[slot] = nullptr;
     c->batch_dev_bytes[slot] = 0;
-    if ((e = cudaMalloc(&c->batch_dev[slot], total * 2)) != cudaSuccess) return cuda_fail(e, "batch tables");
+    if ((e = cudaMalloc(&c->batch_dev[slot], total * 2)) != cudaSuccess) return bail(e, "batch tables");
     c->batch_dev_bytes[slot] = total * 2;
   }
   if (upload > c->batch_host_bytes[slot]) {
     if (c->batch_host[slot]) cudaFreeHost(c->batch_host[slot]);
     c->batch_host[slot] = nullptr;
     c->batch_host_bytes[slot] = 0;
-    if ((e = cudaMallocHost(&c->batch_host[slot], upload * 2)) != cudaSuccess) return cuda_fail(e, "batch staging");
+    if ((e = cudaMallocHost(&c->batch_host[slot], upload * 2)) != cudaSuccess) return bail(e, "batch staging");
     c->batch_host_bytes[slot] = upload * 2;
   }
   if (grp_bytes > c->grp_scratch_bytes[slot]) {
@@ -905,7 +927,7 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
     c->grp_scratch_bytes[slot] = 0;
     const size_t want = std::min(kGroupScratchCap, grp_bytes * 2);
     if ((e = cudaMalloc(reinterpret_cast<void**>(&c->grp_scratch[slot]), want)) != cudaSuccess)
-      return cuda_fail(e, "batch scratch");
+      return bail(e, "batch scratch");
     c->grp_scratch_bytes[slot] = want;
   }
   uint8_t* h = c->batch_host[slot];
@@ -937,15 +959,31 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
     }
   }
   uint8_t* d = c->batch_dev[slot];
+  // Every exit from here on records batch_free[slot] on `s` (the next call on
+  // this slot waits for it before it rewrites the slot's staging and
+  // tables), joins every group stream it forked, and on failure marks the
+  // jobs as not run.
+  auto finish = [&](cudaError_t err, const char* what) -> int {
+    if (err != cudaSuccess)
+      for (size_t i : valid) jobs[i].status = AFRS_ECUDA;
+    cudaError_t re = cudaEventRecord(c->batch_free[slot], s);
+    if (err == cudaSuccess && re != cudaSuccess) {
+      err = re;
+      what = "batch record";
+    }
+    return err == cudaSuccess ? AFRS_OK : cuda_fail(err, what);
+  };
   if ((e = cudaMemcpyAsync(d, h, upload, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-    return cuda_fail(e, "batch upload");
+    return finish(e, "batch upload");
   // Fork the group streams right after the upload, so that the groups run
   // concurrently with the generic kernel below.
   const int nstreams = (int)std::min<size_t>(4, groups.size());
-  if (nstreams && (e = cudaEventRecord(c->grp_fork, s)) != cudaSuccess) return cuda_fail(e, "batch fork");
-  for (int k = 0; k < nstreams; k++)
-    if ((e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_fork, 0)) != cudaSuccess) return cuda_fail(e, "batch fork");
-  if (!bj.empty()) {
+  int forked = 0;
+  const char* what = "batch fork";
+  if (nstreams) e = cudaEventRecord(c->grp_fork, s);
+  for (int k = 0; k < nstreams && e == cudaSuccess; k++)
+    if ((e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_fork, 0)) == cudaSuccess) forked = k + 1;
+  if (e == cudaSuccess && !bj.empty()) {
     afrs::BatchLaunch bl{};
     bl.jobs = reinterpret_cast<const afrs::BatchJob*>(d + o_jobs);
     bl.tasks = reinterpret_cast<const uint2*>(d + o_tasks);
@@ -956,32 +994,35 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
     bl.loc_tab = d + o_loc;
     bl.counter = reinterpret_cast<unsigned*>(d + o_cnt);
     bl.max_rows = max_rows;
-    if ((e = afrs::launch_batch(bl, s)) != cudaSuccess) return cuda_fail(e, "batch launch");
+    e = afrs::launch_batch(bl, s);
+    what = "batch launch";
   }
   // Shape groups are independent: largest first, round-robin over the group
   // streams, after the upload, joined back into `s`.
-  std::vector<size_t> order(groups.size());
-  for (size_t q = 0; q < order.size(); q++) order[q] = q;
-  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
-    return groups[x].count * groups[x].max_ncw * groups[x].n > groups[y].count * groups[y].max_ncw * groups[y].n;
-  });
-  cudaError_t le = cudaSuccess;
-  for (size_t q = 0; q < order.size() && le == cudaSuccess; q++) {
-    const Group& gr = groups[order[q]];
-    cudaStream_t gs = c->grp_stream[q % nstreams];
-    le = gr.op == 0 ? afrs::launch_encode_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs)
-                    : afrs::launch_recover_jobs(gr.n, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
+  if (e == cudaSuccess) {
+    std::vector<size_t> order(groups.size());
+    for (size_t q = 0; q < order.size(); q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+      return groups[x].count * groups[x].max_ncw * groups[x].n > groups[y].count * groups[y].max_ncw * groups[y].n;
+    });
+    for (size_t q = 0; q < order.size() && e == cudaSuccess; q++) {
+      const Group& gr = groups[order[q]];
+      cudaStream_t gs = c->grp_stream[q % nstreams];
+      e = gr.op == 0 ? afrs::launch_encode_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs)
+                     : afrs::launch_recover_jobs(gr.n, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
+      what = "batch group launch";
+    }
   }
   // Join every forked stream, also after a failed launch.
-  for (int k = 0; k < nstreams; k++) {
+  for (int k = 0; k < forked; k++) {
     cudaError_t je = cudaEventRecord(c->grp_join[k], c->grp_stream[k]);
     if (je == cudaSuccess) je = cudaStreamWaitEvent(s, c->grp_join[k], 0);
-    if (e == cudaSuccess) e = je;
+    if (e == cudaSuccess && je != cudaSuccess) {
+      e = je;
+      what = "batch join";
+    }
   }
-  if (le != cudaSuccess) return cuda_fail(le, "batch group launch");
-  if (e != cudaSuccess) return cuda_fail(e, "batch join");
-  if ((e = cudaEventRecord(c->batch_free[slot], s)) != cudaSuccess) return cuda_fail(e, "batch record");
-  return AFRS_OK;
+  return finish(e, what);
 }
 
 }  // extern "C"

@@ -79,6 +79,9 @@ struct ScratchArena {
 // cudaErrorMemoryAllocation.
 cudaError_t launch_encode_special(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s);
 cudaError_t launch_recover_special(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s);
+// Loads the code of every recover kernel launch_recover_special may launch,
+// on the current device, so that no later launch loads code lazily.
+cudaError_t preload_recover_special();
 size_t scratch_bytes_encode(int n, int t, size_t L);
 // Sets the calling thread's afrs_last_error() message.
 void set_last_error(const char* msg);

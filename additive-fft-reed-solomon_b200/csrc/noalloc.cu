@@ -43,7 +43,11 @@ bool pow2(uint32_t v) { return v && !(v & (v - 1)); }
 
 // The array's name is a host-side stand-in, not a device address; the
 // device address is looked up once per device, with that device current.
-int scratch_for_current_device(uint32_t** out) {
+// The same set-up step loads the code of every recover kernel on the device
+// (CUDA otherwise loads a kernel's code at its first launch, which may
+// allocate and is not allowed inside stream capture), so after the first
+// call on a device no call of any shape loads or allocates anything.
+int setup_current_device(uint32_t** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(AFRS_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
@@ -53,6 +57,8 @@ int scratch_for_current_device(uint32_t** out) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return fail(AFRS_ECUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    e = afrs::preload_recover_special();
+    if (e != cudaSuccess) return fail(AFRS_ECUDA, "loading the recover kernels: %s", cudaGetErrorString(e));
     g_scratch_ptr[dev] = static_cast<uint32_t*>(p);
   }
   *out = g_scratch_ptr[dev];
@@ -82,13 +88,11 @@ extern "C" int afrs_recover_dev_noalloc(uint32_t n, uint32_t t, uint8_t* d_recei
                 "shard_len=%zu with n=%u needs %zu bytes of scratch; this entry point has %zu "
                 "(use afrs_recover_dev for larger shards)",
                 shard_len, n, need, kNoAllocScratchBytes);
+  uint32_t* p = nullptr;
+  int r = setup_current_device(&p);
+  if (r) return r;
   afrs::ScratchArena sc{nullptr, 0};
-  if (need) {
-    uint32_t* p = nullptr;
-    int r = scratch_for_current_device(&p);
-    if (r) return r;
-    sc = afrs::ScratchArena{p, kNoAllocScratchBytes};
-  }
+  if (need) sc = afrs::ScratchArena{p, kNoAllocScratchBytes};
   afrs::RecoverArgs a{};
   a.rx = d_received;
   a.L = shard_len;

@@ -1275,6 +1275,22 @@ cudaError_t launch_rec_jobs(RecJob* d, int count, size_t max_ncw, cudaStream_t s
   }
 }
 
+// Loads the module code of the recover kernels of one n (CUDA loads kernel
+// code lazily, at a kernel's first launch, and that load may allocate):
+// querying a kernel's attributes loads it.
+template <int LOGN>
+cudaError_t preload_rec() {
+  cudaFuncAttributes fa;
+  if constexpr (LOGN <= 4) {
+    return cudaFuncGetAttributes(&fa, k_rec_small<LOGN>);
+  } else {
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_rec_b1<LOGN>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_p2<LOGN>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_b3<LOGN>);
+    return e;
+  }
+}
+
 // Scratch bytes a call needs for one batch covering the whole shard
 // (callers may provide less: the launchers then batch the columns).
 inline size_t scratch_full_bytes_enc(int n, int t, size_t L) {
@@ -1289,7 +1305,8 @@ inline size_t scratch_full_bytes_rec(int n, size_t L) { return n >= 32 ? (size_t
   cudaError_t launch_enc_jobs_##LN##_##LT(const EncJob* d, int count, size_t max_ncw, cudaStream_t s);
 #define AFRS_DECLARE_REC(LN)                                                                   \
   cudaError_t launch_rec_##LN(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s); \
-  cudaError_t launch_rec_jobs_##LN(RecJob* d, int count, size_t max_ncw, cudaStream_t s);
+  cudaError_t launch_rec_jobs_##LN(RecJob* d, int count, size_t max_ncw, cudaStream_t s);     \
+  cudaError_t preload_rec_##LN();
 AFRS_DECLARE_ENC(1, 0)
 AFRS_DECLARE_ENC(2, 0)
 AFRS_DECLARE_ENC(2, 1)

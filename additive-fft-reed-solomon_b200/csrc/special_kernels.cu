@@ -94,6 +94,16 @@ cudaError_t launch_recover_special(const RecoverArgs& a, const ScratchArena& sc,
   }
 }
 
+cudaError_t preload_recover_special() {
+  cudaError_t (*const fns[])() = {spec::preload_rec_1, spec::preload_rec_2, spec::preload_rec_3, spec::preload_rec_4,
+                                   spec::preload_rec_5, spec::preload_rec_6, spec::preload_rec_7, spec::preload_rec_8};
+  for (auto f : fns) {
+    cudaError_t e = f();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 size_t scratch_bytes_encode(int n, int t, size_t L) { return spec::scratch_full_bytes_enc(n, t, L); }
 size_t scratch_bytes_recover(int n, size_t L) { return spec::scratch_full_bytes_rec(n, L); }
 

@@ -9,5 +9,6 @@ cudaError_t launch_rec_3(const RecoverArgs& a, const ScratchArena& sc, cudaStrea
 cudaError_t launch_rec_jobs_3(RecJob* d, int count, size_t max_ncw, cudaStream_t s) {
   return launch_rec_jobs<3>(d, count, max_ncw, s);
 }
+cudaError_t preload_rec_3() { return preload_rec<3>(); }
 }  // namespace spec
 }  // namespace afrs

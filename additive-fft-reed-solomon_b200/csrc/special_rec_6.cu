@@ -9,5 +9,6 @@ cudaError_t launch_rec_6(const RecoverArgs& a, const ScratchArena& sc, cudaStrea
 cudaError_t launch_rec_jobs_6(RecJob* d, int count, size_t max_ncw, cudaStream_t s) {
   return launch_rec_jobs<6>(d, count, max_ncw, s);
 }
+cudaError_t preload_rec_6() { return preload_rec<6>(); }
 }  // namespace spec
 }  // namespace afrs

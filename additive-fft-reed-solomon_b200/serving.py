@@ -11,6 +11,13 @@ serves the same requests one call at a time (the per-call path).
 
 Both record, per request, the latency from arrival to completion (host
 clock, completion observed through CUDA events).
+
+Stream order: ``submit`` records an event on the caller's current stream, and
+the stream that runs the request waits on it, so work the caller enqueued on
+the request's buffers before submitting (a fill, a copy) is finished first.
+The buffers are also recorded on the running stream, so that torch's caching
+allocator does not hand their memory to another tensor while the request is
+still on the GPU.
 """
 from __future__ import annotations
 
@@ -31,6 +38,24 @@ class Request(Job):
         super().__init__(job.op, job.n, job.t, job.src, job.dst, job.shard_len, job.positions)
         self.arrival = arrival
         self.done = None
+        self.ready = None  # event on the submitter's stream (mark_submitted)
+
+    def mark_submitted(self) -> None:
+        """Records, on the caller's current stream, the point after which the
+        request's buffers may be used."""
+        import torch
+
+        self.ready = torch.cuda.Event()
+        self.ready.record()
+
+    def enter_stream(self, s) -> None:
+        """Orders stream ``s`` after the submitter's work on the buffers and
+        keeps the buffers' memory from being reused before ``s`` is done."""
+        if self.ready is not None:
+            s.wait_event(self.ready)
+        for buf in (self.src, self.dst):
+            if buf is not None and hasattr(buf, "record_stream"):
+                buf.record_stream(s)
 
     @property
     def latency(self) -> float:
@@ -90,6 +115,7 @@ class BatchServer:
         self.large = PlainServer(device, window=4)
 
     def submit(self, req: Request) -> None:
+        req.mark_submitted()
         if req.nbytes >= self.large_bytes:
             self.large.submit(req)
         else:
@@ -143,6 +169,8 @@ class BatchServer:
                 break
             arr = make_job_array(take)
             s = self.streams[i]
+            for r in take:
+                r.enter_stream(s)
             _check(_lib.lib().afrs_batch_dev(self.ctx.handle, arr, len(take), s.cuda_stream), "afrs_batch_dev")
             for q, r in enumerate(take):
                 r.status = int(arr[q].status)
@@ -168,6 +196,8 @@ class PlainServer:
         self.codecs = {}
 
     def submit(self, req: Request) -> None:
+        if req.ready is None:
+            req.mark_submitted()
         self.queue.append(req)
 
     def pending(self) -> int:
@@ -191,6 +221,7 @@ class PlainServer:
         with torch.cuda.stream(self.stream):
             while self.queue and len(self.inflight) < self.window:
                 r = self.queue.popleft()
+                r.enter_stream(self.stream)
                 c = self._codec(r.n, r.t)
                 if r.op == _lib.AFRS_OP_ENCODE:
                     c.encode_parity(r.src, r.dst, r.shard_len)

@@ -142,8 +142,12 @@ int afrs_batch_dev(afrs_ctx* ctx, afrs_job* jobs, size_t count, void* stream);
  * the process exits); shards that need more (n * ceil(shard_len/1024) * 2 KiB
  * > 32 MiB for n >= 32, e.g. n = 256 with shard_len > 64 KiB) are refused
  * with AFRS_EINVAL and a message in afrs_last_error().  The first call on a
- * device looks up the array's device address (a set-up step), so make it
- * before any stream capture.  All calls share the one array: calls that
+ * device that launches work (valid arguments, 1 <= e <= t, shard_len > 0)
+ * runs a set-up step: it looks up the array's device address and loads the
+ * code of the recover kernels of every n (CUDA otherwise loads a kernel's
+ * code at its first launch, which may allocate).  Make that first call
+ * before any stream capture; after it, calls of any n and shard length
+ * load and allocate nothing.  All calls share the one array: calls that
  * overlap on the GPU (different streams, or different host threads) race and
  * must be ordered by the caller.  No scratch word needs clearing between
  * calls: each call writes every word it reads. */
@@ -166,6 +170,16 @@ const char* afrs_version(void);
 #define AFRS_HOST_STAGED 1
 #define AFRS_HOST_DIRECT 2
 int afrs_ctx_set_staging(afrs_ctx* ctx, size_t window_bytes, size_t merge_bytes, int host_mode);
+
+/* Largest device scratch (bytes) the context's encode and recover calls use
+ * for the rows they keep between kernels; 0 restores the default, 1 GiB,
+ * which is also the maximum.  Shards whose calls need more are processed in
+ * column batches that each fit the cap, so a small cap bounds the context's
+ * device memory at the price of more launches.  Values below 16 KiB (one
+ * colword of an n = 256 recover) are refused with AFRS_EINVAL.  A
+ * diagnostic and memory-budget knob; no counterpart in the reference, whose
+ * calls take a caller-sized workspace (rs/src/codec.rs:241-247, :479-485). */
+int afrs_ctx_set_work_cap(afrs_ctx* ctx, size_t bytes);
 
 /* Number of CUDA kernels this library has launched in this process, over
  * every context and entry point (a diagnostic for benchmarks and tests; no

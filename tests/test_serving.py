@@ -16,8 +16,11 @@ def test_percentiles(afrs):
 
 
 def _requests(afrs, count, seed):
+    """Seeded jobs of config-3 shapes and, per job, the bytes the oracle says
+    its dst must hold afterwards: the parity (encode) or the whole original
+    codeword (recover)."""
     rng = np.random.default_rng(seed)
-    out = []
+    out, expect = [], []
     for i in range(count):
         n = int(rng.choice([32, 64, 128, 256]))
         t = int(rng.choice([4, 8, n // 4, n // 2]))
@@ -28,14 +31,16 @@ def _requests(afrs, count, seed):
         if i % 2 == 0:
             job = afrs.Job.encode(n, t, torch.from_numpy(msg).cuda(), torch.zeros(t * L, dtype=torch.uint8,
                                                                                    device="cuda"), L)
+            expect.append(par)
         else:
             cw = np.concatenate([par, msg])
+            expect.append(cw.copy())
             pos = rng.choice(n, int(rng.integers(1, t + 1)), replace=False).tolist()
             for p in pos:
                 cw[p * L:(p + 1) * L] = 0
             job = afrs.Job.recover(n, t, torch.from_numpy(cw).cuda(), L, pos)
         out.append(job)
-    return out
+    return out, expect
 
 
 def _clone(afrs, j):
@@ -46,7 +51,7 @@ def _clone(afrs, j):
 @pytest.mark.gpu
 def test_result_alone_equals_result_in_the_mix(afrs):
     S = afrs.serving
-    jobs = _requests(afrs, 60, seed=4)
+    jobs, expect = _requests(afrs, 60, seed=4)
     alone = [_clone(afrs, j) for j in jobs]
     reqs = [S.Request(j) for j in jobs]
     arrivals = [i * 2e-5 for i in range(len(reqs))]  # arrivals overlap running batches
@@ -59,16 +64,20 @@ def test_result_alone_equals_result_in_the_mix(afrs):
     for j in alone:  # each request served alone, as a batch of one
         afrs.run_batch([j])
     torch.cuda.synchronize()
-    for r, a in zip(reqs, alone):
+    for r, a, want in zip(reqs, alone, expect):
         assert r.status == a.status
-        assert torch.equal(r.dst, a.dst)  # exact: integer arithmetic, no tolerance
+        # exact: integer arithmetic, no tolerance; the oracle's bytes, served
+        # in the mix and served alone
+        got = r.dst.cpu().numpy()
+        assert (got == want).all()
+        assert torch.equal(r.dst, a.dst)
         assert r.latency >= 0
 
 
 @pytest.mark.gpu
 def test_admission_cap_and_plain_server(afrs):
     S = afrs.serving
-    jobs = _requests(afrs, 30, seed=8)
+    jobs, expect = _requests(afrs, 30, seed=8)
     plain_jobs = [_clone(afrs, j) for j in jobs]
     reqs = [S.Request(j) for j in jobs]
     cap = 3 * max(r.nbytes for r in reqs)
@@ -84,5 +93,6 @@ def test_admission_cap_and_plain_server(afrs):
     preqs = [S.Request(j) for j in plain_jobs]
     pdone, _ = S.serve_open_loop(S.PlainServer(), preqs, [0.0] * len(preqs))
     torch.cuda.synchronize()
-    for r, p in zip(reqs, preqs):
+    for r, p, want in zip(reqs, preqs, expect):
+        assert (r.dst.cpu().numpy() == want).all()
         assert torch.equal(r.dst, p.dst)
