@@ -6,6 +6,7 @@
 #pragma once
 #include "afrs_internal.h"
 #include "gf_device.cuh"
+#include "io.cuh"  // load32 / store32
 
 namespace afrs {
 namespace gtile {
@@ -16,46 +17,6 @@ static __constant__ FieldTables c_field = make_field_tables();
 constexpr int kThreads = 256;
 constexpr int kCW = 8;                    // colwords per CTA (256 byte-columns)
 constexpr int kRowStride = 8 * kCW + 1;   // words per bit-sliced row (+1: bank skew)
-
-// Load 32 bytes of one shard row starting at byte column `col` (zero beyond L).
-__device__ __forceinline__ void load32(const uint8_t* row, size_t col, size_t L, uint32_t (&x)[8]) {
-  const uint8_t* p = row + col;
-  if (col + 32 <= L && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
-    uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
-    uint4 b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
-    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
-    return;
-  }
-#pragma unroll
-  for (int w = 0; w < 8; w++) {
-    uint32_t v = 0;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      size_t c = col + 4 * w + q;
-      uint32_t byte = c < L ? p[4 * w + q] : 0u;
-      v |= byte << (8 * q);
-    }
-    x[w] = v;
-  }
-}
-
-__device__ __forceinline__ void store32(uint8_t* row, size_t col, size_t L, const uint32_t (&x)[8]) {
-  uint8_t* p = row + col;
-  if (col + 32 <= L && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
-    reinterpret_cast<uint4*>(p)[0] = make_uint4(x[0], x[1], x[2], x[3]);
-    reinterpret_cast<uint4*>(p)[1] = make_uint4(x[4], x[5], x[6], x[7]);
-    return;
-  }
-#pragma unroll
-  for (int w = 0; w < 8; w++) {
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      size_t c = col + 4 * w + q;
-      if (c < L) p[4 * w + q] = static_cast<uint8_t>(x[w] >> (8 * q));
-    }
-  }
-}
 
 __device__ __forceinline__ void lds8(const uint32_t* base, int row, int cw, uint32_t (&x)[8]) {
   const uint32_t* r = base + row * kRowStride + cw;
@@ -73,6 +34,7 @@ __device__ __forceinline__ void sts8(uint32_t* base, int row, int cw, const uint
 // pairs rows (i, i + 2^j) inside blocks of 2^(j+1) rows with twiddle
 // s_j(beta + omega_blockstart).  Ends with a barrier.
 static __device__ void transform_smem(uint32_t* s, int k, uint8_t beta, bool inverse, int cw, int pw, int P) {
+  static_assert(kThreads / kCW == 32 && kCW * 4 == 32, "a warp holds 4 pair-workers of 8 colwords");
   const int npairs = k > 0 ? (1 << (k - 1)) : 0;
   for (int step = 0; step < k; step++) {
     const int j = inverse ? step : k - 1 - step;
@@ -84,12 +46,25 @@ static __device__ void transform_smem(uint32_t* s, int k, uint8_t beta, bool inv
       uint32_t a[8], b[8];
       lds8(s, ia, cw, a);
       lds8(s, ia + half, cw, b);
+      // From level 2 up, the pairs of one warp (q = 4 w + 0..3 + 32 i,
+      // aligned groups of 4) lie in one block: the twiddle is warp-uniform
+      // and takes the two-network form; below, each lane has its own.
       if (inverse) {
 #pragma unroll
         for (int p = 0; p < 8; p++) b[p] ^= a[p];
-        if (tw) mul_xor_rt(a, b, tw);
+        if (tw) {
+          if (j >= 2)
+            mul_xor_uniform(a, b, c_field.log[tw]);
+          else
+            mul_xor_rt(a, b, tw);
+        }
       } else {
-        if (tw) mul_xor_rt(a, b, tw);
+        if (tw) {
+          if (j >= 2)
+            mul_xor_uniform(a, b, c_field.log[tw]);
+          else
+            mul_xor_rt(a, b, tw);
+        }
 #pragma unroll
         for (int p = 0; p < 8; p++) b[p] ^= a[p];
       }

@@ -114,6 +114,21 @@ __device__ __forceinline__ void static_for(F&& f) {
   static_for_impl(std::make_integer_sequence<int, N>{}, static_cast<F&&>(f));
 }
 
+// Runtime v in [LO, HI] -> f(integral_constant<v>) by binary search; v is
+// warp-uniform at every call site, so the branches do not diverge.
+template <int LO, int HI, typename F>
+__device__ __forceinline__ void dispatch(int v, F&& f) {
+  if constexpr (LO == HI) {
+    f(std::integral_constant<int, LO>{});
+  } else {
+    constexpr int MID = (LO + HI) / 2;
+    if (v <= MID)
+      dispatch<LO, MID>(v, f);
+    else
+      dispatch<MID + 1, HI>(v, f);
+  }
+}
+
 // ---- bit-sliced primitives ----------------------------------------------
 using Planes = uint32_t[8];
 
@@ -156,6 +171,26 @@ __host__ __device__ __forceinline__ void mul_xor_rt(uint32_t (&acc)[8], const ui
     for (int i = 0; i < 8; i++) acc[i] ^= cur[i] & m;
     if (j < 7) xtime(cur);
   }
+}
+
+// acc ^= c * b for a constant c = g^lg (g = 2, lg = log c in [0, 254]) that
+// is the same in every lane of the warp: lg = 16 h + l and c = g^(16 h) g^l,
+// two compile-time XOR networks picked from 16 each (about 36 LOP3 instead
+// of mul_xor_rt's ~85, plus eight uniform branches).
+__device__ __forceinline__ void mul_xor_uniform(uint32_t (&acc)[8], const uint32_t (&b)[8], int lg) {
+  uint32_t y[8];
+  dispatch<0, 15>(lg >> 4, [&](auto h) {
+    constexpr uint8_t C = kField.exp[16 * decltype(h)::value];
+    if constexpr (C == 1) {
+#pragma unroll
+      for (int p = 0; p < 8; p++) y[p] = b[p];
+    } else {
+#pragma unroll
+      for (int p = 0; p < 8; p++) y[p] = 0;
+      mul_xor_c<C>(y, b);
+    }
+  });
+  dispatch<0, 15>(lg & 15, [&](auto l) { mul_xor_c<kField.exp[decltype(l)::value]>(acc, y); });
 }
 
 // 8x8 bit transpose in each byte lane of eight words.  Applied to eight

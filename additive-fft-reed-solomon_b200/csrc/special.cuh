@@ -107,21 +107,6 @@ __device__ __forceinline__ void one_plus_derivative(uint32_t (&x)[NR][8]) {
   });
 }
 
-// Runtime v in [LO, HI] -> f(integral_constant<v>) by binary search; v is
-// warp-uniform at every call site, so the branches do not diverge.
-template <int LO, int HI, typename F>
-__device__ __forceinline__ void dispatch(int v, F&& f) {
-  if constexpr (LO == HI) {
-    f(std::integral_constant<int, LO>{});
-  } else {
-    constexpr int MID = (LO + HI) / 2;
-    if (v <= MID)
-      dispatch<LO, MID>(v, f);
-    else
-      dispatch<MID + 1, HI>(v, f);
-  }
-}
-
 // Bit-sliced shared-memory tile: row r, plane p, colword w at
 // sm[(r * 8 + p) * CW + w]; a warp reading one (row, plane) over 32 colwords
 // touches 32 consecutive words.
