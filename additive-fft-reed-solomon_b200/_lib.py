@@ -19,6 +19,11 @@ _u8p = ctypes.c_void_p
 _sz = ctypes.c_size_t
 _u32 = ctypes.c_uint32
 
+AFRS_ROUTE_TABLE = 0
+AFRS_ROUTE_GENERIC = 1
+AFRS_ROUTE_SPECIAL = 2
+AFRS_ROUTE_SPECIAL_SPLIT = 3
+
 AFRS_OP_ENCODE = 0
 AFRS_OP_RECOVER = 1
 
@@ -40,6 +45,7 @@ SIGNATURES = {
     "afrs_kernel_launches": (ctypes.c_uint64, []),
     "afrs_ctx_set_staging": (ctypes.c_int, [ctypes.c_void_p, _sz, _sz, ctypes.c_int]),
     "afrs_ctx_set_work_cap": (ctypes.c_int, [ctypes.c_void_p, _sz]),
+    "afrs_ctx_set_route": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "afrs_staged_bytes": (None, [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "afrs_encode": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _u8p, _sz, ctypes.c_int]),
     "afrs_recover": (ctypes.c_int, [ctypes.c_void_p, _u32, _u32, _u8p, _sz, _u8p, _sz]),

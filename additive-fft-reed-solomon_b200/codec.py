@@ -69,6 +69,11 @@ class Context:
         restores the default."""
         _check(_lib.lib().afrs_ctx_set_work_cap(self._h, int(nbytes)), "afrs_ctx_set_work_cap")
 
+    def set_route(self, route: int) -> None:
+        """Kernel family of the context's per-call encodes and recovers
+        (afrs_ctx_set_route): _lib.AFRS_ROUTE_TABLE (default) or a forced one."""
+        _check(_lib.lib().afrs_ctx_set_route(self._h, int(route)), "afrs_ctx_set_route")
+
     def close(self) -> None:
         if self._h:
             _lib.lib().afrs_ctx_destroy(self._h)

@@ -23,6 +23,7 @@ struct afrs_ctx {
   uint32_t* work;  // bit-sliced intermediate rows of the phase kernels
   size_t work_bytes;
   size_t work_cap;  // largest phase scratch used per call (afrs_ctx_set_work_cap)
+  int route;        // forced per-call route (afrs_ctx_set_route): -1 = tuned table
   cudaEvent_t work_free;  // recorded after each use of `work`
   // Descriptor tables of afrs_batch_dev, two slots so that one batch can be
   // prepared while the previous one runs.
@@ -157,25 +158,36 @@ cudaError_t release_work(afrs_ctx* c, cudaStream_t s) {
   return capturing(s) ? cudaSuccess : cudaEventRecord(c->work_free, s);
 }
 
-// Shapes where the one-launch generic kernel is faster per call than the
-// specialised ones (measured on a B200, codewords up to 4 MiB): encodes with
+// Built-in routing, used where the tuned table (route.cu) has no entry:
+// shapes where the one-launch generic kernel was measured faster per call
+// than the specialised ones (B200, codewords up to 4 MiB): encodes with
 // t = 16 and n >= 32 (n = 32, 1 KiB shards: 6.2 vs 27.6 us; n = 64: 10 vs
 // 26.5 us; n = 256: 33 vs 44 us), and encodes with t >= 32 and n <= 64, where
 // three phase launches cost more than the work (n = 64, t = 32, 1 KiB: 8.2
 // vs 13.9 us).  Beyond 4 MiB the generic kernel's time grows with the bytes
 // and the specialised ones win (n = 32, t = 16, 1 MiB shards: 68 vs 28 us).
-// The generic kernel takes compact rows (no row pitch).
 bool generic_encode_wins(const afrs::EncodeArgs& a) {
-  if (a.pitch && a.pitch != a.L) return false;
   if ((size_t)a.n * a.L > ((size_t)4 << 20)) return false;
   return a.t <= 16 ? a.t == 16 && a.n >= 32 : a.n <= 64;
 }
 
-int launch_encode(afrs_ctx* c, const afrs::EncodeArgs& a, cudaStream_t s) {
-  if (generic_encode_wins(a)) {
-    cudaError_t e = afrs::launch_encode_generic(a, s);
+// Route of one encode: the context's forced route, else the tuned table,
+// else the built-in rule.  The generic kernel takes compact rows only.
+int encode_route(const afrs_ctx* c, const afrs::EncodeArgs& a) {
+  const bool compact = !a.pitch || a.pitch == a.L;
+  int r = c->route >= 0 ? c->route : afrs::route_encode(a.n, a.t, a.L);
+  if (r < 0) return compact && generic_encode_wins(a) ? afrs::kRouteGeneric : -1;
+  return r == afrs::kRouteGeneric && !compact ? afrs::kRouteSpecial : r;
+}
+
+int launch_encode(afrs_ctx* c, const afrs::EncodeArgs& a0, cudaStream_t s) {
+  const int route = encode_route(c, a0);
+  if (route == afrs::kRouteGeneric) {
+    cudaError_t e = afrs::launch_encode_generic(a0, s);
     return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "encode launch");
   }
+  afrs::EncodeArgs a = a0;
+  if (route >= 0) a.layout = route == afrs::kRouteSpecialSplit ? 1 : 0;  // else the launcher's rule
   afrs::ScratchArena sc{nullptr, 0};
   cudaError_t e = cudaSuccess;
   const size_t need = afrs::scratch_bytes_encode(a.n, a.t, a.L);
@@ -186,16 +198,22 @@ int launch_encode(afrs_ctx* c, const afrs::EncodeArgs& a, cudaStream_t s) {
   return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "encode launch");
 }
 
-// Recovers with n = 16 up to 4 MiB: the one-launch generic kernel is faster
-// per call than the specialised whole-column kernel there (1 KiB shards: 10.3
-// vs 24.6 us; 256 KiB: 24.7 vs 26.9 us; 1 MiB: 74 vs 27 us).
+// Built-in rule where the table has no entry: recovers with n = 16 up to
+// 4 MiB take the one-launch generic kernel (1 KiB shards: 10.3 vs 24.6 us;
+// 256 KiB: 24.7 vs 26.9 us; 1 MiB: 74 vs 27 us).
 bool generic_recover_wins(const afrs::RecoverArgs& a) {
-  if (a.pitch && a.pitch != a.L) return false;
   return a.n == 16 && (size_t)a.n * a.L <= ((size_t)4 << 20);
 }
 
+int recover_route(const afrs_ctx* c, const afrs::RecoverArgs& a) {
+  const bool compact = !a.pitch || a.pitch == a.L;
+  int r = c->route >= 0 ? c->route : afrs::route_recover(a.n, a.L);
+  if (r < 0) r = generic_recover_wins(a) ? afrs::kRouteGeneric : afrs::kRouteSpecial;
+  return r == afrs::kRouteGeneric && !compact ? afrs::kRouteSpecial : r;
+}
+
 int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
-  if (generic_recover_wins(a)) {
+  if (recover_route(c, a) == afrs::kRouteGeneric) {
     cudaError_t e = afrs::launch_recover_generic(a, s);
     return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "recover launch");
   }
@@ -443,6 +461,15 @@ int afrs_ctx_set_work_cap(afrs_ctx* c, size_t bytes) {
   return AFRS_OK;
 }
 
+int afrs_ctx_set_route(afrs_ctx* c, int route) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (route < AFRS_ROUTE_TABLE || route > AFRS_ROUTE_SPECIAL_SPLIT)
+    return fail(AFRS_EINVAL, "route %d is not an AFRS_ROUTE_* value", route);
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->route = route == AFRS_ROUTE_TABLE ? -1 : route - AFRS_ROUTE_GENERIC;
+  return AFRS_OK;
+}
+
 uint64_t afrs_kernel_launches(void) { return afrs::g_launches.load(std::memory_order_relaxed); }
 
 void afrs_staged_bytes(uint64_t* h2d, uint64_t* d2h) {
@@ -468,6 +495,7 @@ int afrs_ctx_create(int device, afrs_ctx** out) {
   c->work = nullptr;
   c->work_bytes = 0;
   c->work_cap = kWorkCap;
+  c->route = -1;
   for (int i = 0; i < 2; i++) {
     c->batch_dev[i] = nullptr;
     c->batch_dev_bytes[i] = 0;

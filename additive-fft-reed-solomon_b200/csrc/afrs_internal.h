@@ -24,6 +24,9 @@ struct EncodeArgs {
   int n, t;
   int accumulate;
   size_t pitch = 0;  // bytes between rows of msg and parity; 0 = L
+  // t <= 16 encodes with several chunks: 1 = the warps of a CTA split one
+  // slice's chunks, 0 = one warp per slice, -1 = chosen by the built-in rule.
+  int layout = -1;
 };
 template <class A>
 __host__ __device__ inline size_t row_pitch(const A& a) {
@@ -65,6 +68,16 @@ cudaError_t launch_scale(const uint8_t* src, uint8_t* dst, size_t len, uint8_t c
 // dst ^= src; *count += nonzero bytes of src (byte streams, any alignment).
 cudaError_t launch_xor_into(uint8_t* dst, const uint8_t* src, size_t len, cudaStream_t s);
 cudaError_t launch_count_nonzero(const uint8_t* src, size_t len, unsigned long long* count, cudaStream_t s);
+
+// Per-call kernel routes (route.cu): the tuned table (route_table.inc,
+// written by tune.py) for a shape and shard-length bucket, or -1 when it has
+// no entry (the built-in rules decide).
+enum Route : int { kRouteGeneric = 0, kRouteSpecial = 1, kRouteSpecialSplit = 2 };
+int route_encode(int n, int t, size_t L);
+int route_recover(int n, size_t L);
+// Bucket of a shard length in the table: 0 for L <= 64, else ceil(log2 L) - 6;
+// -1 beyond the largest tuned length.
+int route_bucket(size_t L);
 
 // Device scratch for the phase kernels (bit-sliced intermediate rows).
 struct ScratchArena {

@@ -34,7 +34,6 @@ __device__ __forceinline__ void sts8(uint32_t* base, int row, int cw, const uint
 // pairs rows (i, i + 2^j) inside blocks of 2^(j+1) rows with twiddle
 // s_j(beta + omega_blockstart).  Ends with a barrier.
 static __device__ void transform_smem(uint32_t* s, int k, uint8_t beta, bool inverse, int cw, int pw, int P) {
-  static_assert(kThreads / kCW == 32 && kCW * 4 == 32, "a warp holds 4 pair-workers of 8 colwords");
   const int npairs = k > 0 ? (1 << (k - 1)) : 0;
   for (int step = 0; step < k; step++) {
     const int j = inverse ? step : k - 1 - step;
@@ -46,25 +45,12 @@ static __device__ void transform_smem(uint32_t* s, int k, uint8_t beta, bool inv
       uint32_t a[8], b[8];
       lds8(s, ia, cw, a);
       lds8(s, ia + half, cw, b);
-      // From level 2 up, the pairs of one warp (q = 4 w + 0..3 + 32 i,
-      // aligned groups of 4) lie in one block: the twiddle is warp-uniform
-      // and takes the two-network form; below, each lane has its own.
       if (inverse) {
 #pragma unroll
         for (int p = 0; p < 8; p++) b[p] ^= a[p];
-        if (tw) {
-          if (j >= 2)
-            mul_xor_uniform(a, b, c_field.log[tw]);
-          else
-            mul_xor_rt(a, b, tw);
-        }
+        if (tw) mul_xor_rt(a, b, tw);
       } else {
-        if (tw) {
-          if (j >= 2)
-            mul_xor_uniform(a, b, c_field.log[tw]);
-          else
-            mul_xor_rt(a, b, tw);
-        }
+        if (tw) mul_xor_rt(a, b, tw);
 #pragma unroll
         for (int p = 0; p < 8; p++) b[p] ^= a[p];
       }

@@ -173,26 +173,6 @@ __host__ __device__ __forceinline__ void mul_xor_rt(uint32_t (&acc)[8], const ui
   }
 }
 
-// acc ^= c * b for a constant c = g^lg (g = 2, lg = log c in [0, 254]) that
-// is the same in every lane of the warp: lg = 16 h + l and c = g^(16 h) g^l,
-// two compile-time XOR networks picked from 16 each (about 36 LOP3 instead
-// of mul_xor_rt's ~85, plus eight uniform branches).
-__device__ __forceinline__ void mul_xor_uniform(uint32_t (&acc)[8], const uint32_t (&b)[8], int lg) {
-  uint32_t y[8];
-  dispatch<0, 15>(lg >> 4, [&](auto h) {
-    constexpr uint8_t C = kField.exp[16 * decltype(h)::value];
-    if constexpr (C == 1) {
-#pragma unroll
-      for (int p = 0; p < 8; p++) y[p] = b[p];
-    } else {
-#pragma unroll
-      for (int p = 0; p < 8; p++) y[p] = 0;
-      mul_xor_c<C>(y, b);
-    }
-  });
-  dispatch<0, 15>(lg & 15, [&](auto l) { mul_xor_c<kField.exp[decltype(l)::value]>(acc, y); });
-}
-
 // 8x8 bit transpose in each byte lane of eight words.  Applied to eight
 // words of raw bytes (word w = bytes 4w..4w+3 of a 32-byte run) it yields
 // the planes: plane b, bit 8q+w = bit b of byte 4w+q.  It is an involution,

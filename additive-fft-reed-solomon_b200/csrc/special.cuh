@@ -134,23 +134,9 @@ __device__ __forceinline__ void gstore(uint8_t* base, size_t row, size_t pitch, 
   store_cw(base + row * pitch, L, w, x);
 }
 
-// y <- c * y for c = g^a (g = 2), a in [0, 254] uniform across the CTA:
-// a = 16 h + l and c = g^l * g^(16 h), two multiplies by compile-time
-// constants picked from 16 each (32 XOR networks of code in total).
-template <int C>
-__device__ __forceinline__ void mul_by_c(uint32_t (&y)[8]) {
-  if constexpr (C != 1) {
-    uint32_t r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    mul_xor_c<static_cast<uint8_t>(C)>(r, y);
-#pragma unroll
-    for (int p = 0; p < 8; p++) y[p] = r[p];
-  }
-}
-__device__ __forceinline__ void scale_log(uint32_t (&y)[8], int a) {
-  dispatch<0, 15>(a >> 4, [&](auto h) { mul_by_c<kField.exp[16 * decltype(h)::value]>(y); });
-  dispatch<0, 15>(a & 15, [&](auto l) { mul_by_c<kField.exp[decltype(l)::value]>(y); });
-}
-
+// y <- c * y for a runtime constant c (branch-free shift-and-add; measured
+// faster in the bottom passes than picking two compile-time networks by the
+// logarithm of c, whose uniform branches cost more than the XORs they save).
 __device__ __forceinline__ void scale_rt(uint32_t (&x)[8], uint32_t c) {
   uint32_t r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   mul_xor_rt(r, x, c);
@@ -911,7 +897,7 @@ __device__ __forceinline__ void rec_b1_body(const RecoverArgs& a, const Batch& b
       uint32_t y[8];
       s_get(st, i, threadIdx.x, y);
       transpose8f(y, km);
-      scale_log(y, loc.lam[row0 + i]);
+      scale_rt(y, c_tab.exp[loc.lam[row0 + i]]);
       s_put(st, i, threadIdx.x, y);
     }
 #pragma unroll
@@ -1011,7 +997,7 @@ __device__ __forceinline__ void rec_b3_body(const RecoverArgs& a, const Batch& b
       if (!loc.er[r]) continue;
       uint32_t y[8];
       s_get(st, i, tid, y);
-      scale_log(y, loc.ilp[r]);
+      scale_rt(y, c_tab.exp[loc.ilp[r]]);
       gstore(a.rx, r, row_pitch(a), a.L, bt.cw0 + q.w, y, km);
     }
   }
@@ -1121,8 +1107,9 @@ inline size_t batch_colwords(size_t rows_per_buffer, int buffers, size_t scratch
 template <int LOGN, int LOGT>
 cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s) {
   if constexpr (LOGT <= 4) {
+    constexpr int C = ((1 << LOGN) >> LOGT) - 1;
     const size_t slices = (a.L + 1023) / 1024;
-    const bool split = enc_small_split<LOGN, LOGT>(slices);
+    const bool split = a.layout >= 0 ? (a.layout != 0 && C > 1) : enc_small_split<LOGN, LOGT>(slices);
     const size_t smem = enc_small_smem<LOGN, LOGT>(split);
     auto fn = split ? k_enc_small<LOGN, LOGT, true> : k_enc_small<LOGN, LOGT, false>;
     if (smem > (48 << 10)) {

@@ -215,7 +215,8 @@ def main():
     ap.add_argument("--pairs", type=int, default=2, help="stream pairs the steps go to round-robin")
     ap.add_argument("--no-graphs", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
     ap.add_argument("--e2e-pairs", type=int, default=3, help="host thread pairs (encode + recover) of the e2e line")
-    ap.add_argument("--workload", default="codeword", choices=["codeword", "small", "batched", "serving", "large"])
+    ap.add_argument("--workload", default="codeword", choices=["codeword", "small", "batched", "serving", "large", "kernels"])
+    ap.add_argument("--shard-len", type=int, default=0, help="--workload large: shard length (default 4 MiB)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

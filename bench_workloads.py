@@ -12,6 +12,12 @@
   large    n=256, k=224 (t=32), 4 MiB shards (1 GiB codeword): encode, then
            recover 32 erasures (a) inside the message shards and (b) as one
            contiguous run, with a bit-exact round-trip check on device
+  kernels  every kernel family once at about 16 MiB per codeword (the
+           per-kernel profiling driver): the t <= 16 encode kernel in both
+           layouts, the generic encode and recover kernels, the n <= 16
+           recover kernel, the phase kernels of n = 256 with t = 32, and the
+           batched path's generic persistent kernel and grouped kernels;
+           each checked against the oracle, timed with CUDA events
 
 Bytes are n*L per codeword operation.  Data are synthetic (seeded).
 """
@@ -218,7 +224,7 @@ def run_large(args):
     import torch
 
     afrs = _pkg()
-    n, t, L = 256, 32, 4 << 20
+    n, t, L = 256, 32, args.shard_len or (4 << 20)
     k = n - t
     g = torch.Generator(device="cuda")
     g.manual_seed(3)
@@ -238,7 +244,7 @@ def run_large(args):
     rng = np.random.default_rng(1)
     patterns = {"a_in_message": sorted(rng.choice(np.arange(32, 256), 32, replace=False).tolist()),
                 "b_contiguous": list(range(100, 132))}
-    out = {"workload": "large: n=256 k=224 t=32 L=4MiB (1 GiB codeword)",
+    out = {"workload": f"large: n=256 k=224 t=32 L={L} ({n * L >> 20} MiB codeword)",
            "encode": {"ms": round(enc_ms, 3), "GB/s": round(n * L / enc_ms / 1e6, 2)}}
     rx = torch.empty_like(cw)
     for name, pos in patterns.items():
@@ -260,5 +266,123 @@ def run_large(args):
     print(json.dumps(out), flush=True)
 
 
+def run_kernels(args):
+    import torch
+
+    from oracle import oracle
+
+    afrs = _pkg()
+    lib = afrs._lib
+    reps = max(3, min(args.steps, 50))
+    out = {"workload": "kernels: each kernel family once at ~16 MiB per codeword (bytes = n * L per operation)"}
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        a, b = _events()
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def encode_case(name, n, t, L, route, kernels):
+        msg = oracle.random_bytes((n - t) * L, n + t)
+        ref = np.zeros(t * L, np.uint8)
+        oracle.encode_systematic_sharded(n, t, msg, ref, L)
+        ctx = afrs.Context(0)
+        ctx.set_route(route)
+        codec = afrs.Codec(n, t, context=ctx)
+        d_msg, d_par = torch.from_numpy(msg).cuda(), torch.zeros(t * L, dtype=torch.uint8, device="cuda")
+        ms = timed(lambda: codec.encode_parity(d_msg, d_par, L))
+        ok = bool((d_par.cpu().numpy() == ref).all())
+        out[name] = {"n": n, "t": t, "L": L, "kernels": kernels, "us": round(ms * 1e3, 2),
+                     "GB/s": round(n * L / ms / 1e6, 1), "bit_exact": ok}
+        ctx.close()
+
+    def recover_case(name, n, t, L, route, kernels):
+        msg = oracle.random_bytes((n - t) * L, n * 7 + t)
+        par = np.zeros(t * L, np.uint8)
+        oracle.encode_systematic_sharded(n, t, msg, par, L)
+        cw = np.concatenate([par, msg])
+        pos = sorted(np.random.default_rng(n).choice(n, t, replace=False).tolist())
+        rx = cw.copy()
+        for p in pos:
+            rx[p * L:(p + 1) * L] = 0
+        ctx = afrs.Context(0)
+        ctx.set_route(route)
+        codec = afrs.Codec(n, t, context=ctx)
+        d = torch.from_numpy(rx).cuda()
+        ms = timed(lambda: codec.recover_erasure_shards(d, None, L, pos))
+        ok = bool((d.cpu().numpy() == cw).all())
+        out[name] = {"n": n, "t": t, "e": t, "L": L, "kernels": kernels, "us": round(ms * 1e3, 2),
+                     "GB/s": round(n * L / ms / 1e6, 1), "bit_exact": ok}
+        ctx.close()
+
+    encode_case("enc_small_one_warp_per_slice", 32, 16, 524288, lib.AFRS_ROUTE_SPECIAL, "k_enc_small<5,4,false>")
+    encode_case("enc_small_split", 256, 4, 65536, lib.AFRS_ROUTE_SPECIAL_SPLIT, "k_enc_small<8,2,true>")
+    encode_case("encode_generic", 64, 32, 262144, lib.AFRS_ROUTE_GENERIC, "k_encode_generic")
+    encode_case("encode_phases_t32", 256, 32, 65536, lib.AFRS_ROUTE_SPECIAL, "k_enc_b1/p2/b3<8,5>")
+    recover_case("recover_generic", 16, 8, 1 << 20, lib.AFRS_ROUTE_GENERIC, "k_recover_generic")
+    recover_case("rec_small", 16, 8, 1 << 20, lib.AFRS_ROUTE_SPECIAL, "k_rec_small<4>")
+    recover_case("recover_phases_n64", 64, 32, 262144, lib.AFRS_ROUTE_SPECIAL, "k_rec_b1/p2/b3<6>")
+
+    # Batched path: 256 small mixed jobs share the generic persistent kernel
+    # (every shape group is below the grouping threshold); two large shape
+    # groups run the grouped kernels.
+    def batch_case(name, jobs, refs, kernels):
+        total = sum(j.nbytes for j in jobs)
+        ms = timed(lambda: afrs.run_batch(jobs))
+        ok = all(bool((j.dst.cpu().numpy() == r).all()) for j, r in zip(jobs, refs))
+        out[name] = {"jobs": len(jobs), "bytes": total, "kernels": kernels, "us": round(ms * 1e3, 2),
+                     "GB/s": round(total / ms / 1e6, 1), "bit_exact": ok}
+
+    rng = np.random.default_rng(11)
+    jobs, refs = [], []
+    for i in range(256):
+        n, t, L = int(rng.choice([32, 64])), 8, int(rng.choice([256, 512, 1024]))
+        msg = oracle.random_bytes((n - t) * L, 5000 + i)
+        par = np.zeros(t * L, np.uint8)
+        oracle.encode_systematic_sharded(n, t, msg, par, L)
+        if i % 2 == 0:
+            jobs.append(afrs.Job.encode(n, t, torch.from_numpy(msg).cuda(),
+                                        torch.zeros(t * L, dtype=torch.uint8, device="cuda"), L))
+            refs.append(par)
+        else:
+            cw = np.concatenate([par, msg])
+            pos = rng.choice(n, int(rng.integers(1, t + 1)), replace=False).tolist()
+            rx = cw.copy()
+            for p in pos:
+                rx[p * L:(p + 1) * L] = 0
+            jobs.append(afrs.Job.recover(n, t, torch.from_numpy(rx).cuda(), L, pos))
+            refs.append(cw)
+    batch_case("batch_generic", jobs, refs, "k_batch_locator, k_batch")
+    jobs, refs = [], []
+    for i in range(64):
+        enc = i % 2 == 0
+        n, t, L = (128, 32, 2048) if enc else (128, 64, 2048)
+        msg = oracle.random_bytes((n - t) * L, 7000 + i)
+        par = np.zeros(t * L, np.uint8)
+        oracle.encode_systematic_sharded(n, t, msg, par, L)
+        if enc:
+            jobs.append(afrs.Job.encode(n, t, torch.from_numpy(msg).cuda(),
+                                        torch.zeros(t * L, dtype=torch.uint8, device="cuda"), L))
+            refs.append(par)
+        else:
+            cw = np.concatenate([par, msg])
+            pos = sorted(rng.choice(n, t, replace=False).tolist())
+            rx = cw.copy()
+            for p in pos:
+                rx[p * L:(p + 1) * L] = 0
+            jobs.append(afrs.Job.recover(n, t, torch.from_numpy(rx).cuda(), L, pos))
+            refs.append(cw)
+    batch_case("batch_grouped", jobs, refs,
+               "k_enc_b1/p2/b3_jobs<7,5>, k_rec_jobs_locator, k_rec_b1/p2/b3_jobs<7>")
+    print(json.dumps(out), flush=True)
+
+
 def run(name, args):
-    return {"small": run_small, "batched": run_batched, "serving": run_serving, "large": run_large}[name](args)
+    return {"small": run_small, "batched": run_batched, "serving": run_serving, "large": run_large,
+            "kernels": run_kernels}[name](args)

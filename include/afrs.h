@@ -181,6 +181,25 @@ int afrs_ctx_set_staging(afrs_ctx* ctx, size_t window_bytes, size_t merge_bytes,
  * calls take a caller-sized workspace (rs/src/codec.rs:241-247, :479-485). */
 int afrs_ctx_set_work_cap(afrs_ctx* ctx, size_t bytes);
 
+/* Kernel family of the context's per-call encodes and recovers.
+ * AFRS_ROUTE_TABLE (default): per shape and shard length, the family the
+ * library's tuned route table names (measured on a B200 by tune.py in the
+ * package directory), and built-in rules where it names none.  The others
+ * force one family, for tuning and diagnostics: GENERIC, the one-launch
+ * kernel with runtime twiddles (rows must be compact; calls on host buffers
+ * whose windows use a row pitch keep the specialised kernels); SPECIAL, the
+ * kernels with compile-time twiddles, t <= 16 encodes with one warp per
+ * 1024-column slice; SPECIAL_SPLIT, the same with the warps of a CTA
+ * splitting one slice's chunks (t <= 16 encodes with n > 2t; otherwise as
+ * SPECIAL).  Results are identical on every route.  No counterpart in the
+ * reference, whose kernel choice is a build-time CPU feature test
+ * (rs/build.rs:628-646). */
+#define AFRS_ROUTE_TABLE 0
+#define AFRS_ROUTE_GENERIC 1
+#define AFRS_ROUTE_SPECIAL 2
+#define AFRS_ROUTE_SPECIAL_SPLIT 3
+int afrs_ctx_set_route(afrs_ctx* ctx, int route);
+
 /* Number of CUDA kernels this library has launched in this process, over
  * every context and entry point (a diagnostic for benchmarks and tests; no
  * counterpart in the reference). */
