@@ -6,7 +6,7 @@ vkomenda/additive-fft-reed-solomon.  The compute lives in libafrs_b200.so
 reference codec API.
 """
 from ._lib import LIB_PATH, build, lib  # noqa: F401
-from .codec import AfrsError, Codec, Context, Job, fft_sharded, ifft_sharded, run_batch, scale  # noqa: F401
+from .codec import AfrsError, BatchPlan, Codec, Context, Job, fft_sharded, ifft_sharded, run_batch, scale  # noqa: F401
 
 # The reference's type names for the same codec (rs/src/lib.rs:20-45).
 Rs = Codec

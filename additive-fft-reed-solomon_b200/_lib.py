@@ -59,6 +59,10 @@ SIGNATURES = {
     "afrs_scale_dev": (ctypes.c_int, [ctypes.c_void_p, _u8p, _u8p, _sz, ctypes.c_uint8, ctypes.c_void_p]),
     "afrs_recover_dev_noalloc": (ctypes.c_int, [_u32, _u32, _u8p, _sz, _u8p, _sz, ctypes.c_void_p]),
     "afrs_batch_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AfrsJob), _sz, ctypes.c_void_p]),
+    "afrs_batch_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AfrsJob), _sz,
+                                              ctypes.POINTER(ctypes.c_void_p)]),
+    "afrs_batch_plan_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "afrs_batch_plan_destroy": (None, [ctypes.c_void_p]),
 }
 
 

@@ -26,7 +26,7 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["AfrsError", "Context", "Codec", "Job", "run_batch", "fft_sharded", "ifft_sharded", "scale"]
+__all__ = ["AfrsError", "Context", "Codec", "Job", "run_batch", "BatchPlan", "fft_sharded", "ifft_sharded", "scale"]
 
 
 class AfrsError(RuntimeError):
@@ -246,11 +246,7 @@ class Job:
         return self.n * self.shard_len
 
 
-def run_batch(jobs, device: int = 0, stream=None) -> list:
-    """Enqueue every job in one batched launch (afrs_batch_dev) on the
-    current torch stream (or ``stream``); returns the per-job statuses."""
-    import torch
-
+def _job_array(jobs):
     arr = (_lib.AfrsJob * max(len(jobs), 1))()
     for i, j in enumerate(jobs):
         a = arr[i]
@@ -260,6 +256,15 @@ def run_batch(jobs, device: int = 0, stream=None) -> list:
             a.positions[q] = p
         a.src = _dev_ptr(j.src) if j.src is not None else None
         a.dst = _dev_ptr(j.dst) if j.dst is not None else None
+    return arr
+
+
+def run_batch(jobs, device: int = 0, stream=None) -> list:
+    """Enqueue every job in one batched launch (afrs_batch_dev) on the
+    current torch stream (or ``stream``); returns the per-job statuses."""
+    import torch
+
+    arr = _job_array(jobs)
     ctx = Context.get(device)
     s = stream if stream is not None else torch.cuda.current_stream(device)
     _check(_lib.lib().afrs_batch_dev(ctx.handle, arr, len(jobs), s.cuda_stream), "afrs_batch_dev")
@@ -268,3 +273,40 @@ def run_batch(jobs, device: int = 0, stream=None) -> list:
         j.status = int(arr[i].status)
         out.append(j.status)
     return out
+
+
+class BatchPlan:
+    """Jobs prepared once (afrs_batch_plan_create: validation, grouping and
+    descriptor tables copied to the device) and launched any number of times
+    with ``launch()`` (afrs_batch_plan_launch: kernels only, so the launch
+    can be captured into a CUDA graph).  The plan runs on the jobs' buffers;
+    it keeps references to them.  Launches of one plan must not overlap."""
+
+    def __init__(self, jobs, device: int = 0, context: "Context | None" = None):
+        self.jobs = list(jobs)
+        self.ctx = context if context is not None else Context.get(device)
+        arr = _job_array(self.jobs)
+        self._h = ctypes.c_void_p()
+        _check(_lib.lib().afrs_batch_plan_create(self.ctx.handle, arr, len(self.jobs), ctypes.byref(self._h)),
+               "afrs_batch_plan_create")
+        self.statuses = []
+        for i, j in enumerate(self.jobs):
+            j.status = int(arr[i].status)
+            self.statuses.append(j.status)
+
+    def launch(self, stream=None) -> None:
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream()
+        _check(_lib.lib().afrs_batch_plan_launch(self._h, s.cuda_stream), "afrs_batch_plan_launch")
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().afrs_batch_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -789,10 +789,12 @@ int afrs_scale_dev(afrs_ctx* c, const uint8_t* src, uint8_t* dst, size_t len, ui
   return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "scale launch");
 }
 
-static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+}  // extern "C"
 
-// Scratch of one batch slot's grouped launches; jobs beyond it take the
-// generic persistent kernel.
+namespace {
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
 constexpr size_t kGroupScratchCap = (size_t)1 << 30;
 // Smallest shape group (sum of n * shard_len) worth its own launches.
 constexpr size_t kGroupMinBytes = (size_t)8 << 20;
@@ -801,21 +803,36 @@ constexpr size_t kGroupMinBytes = (size_t)8 << 20;
 struct GroupedJob {
   size_t job;      // index into the caller's array
   int op, n, t;    // shape key
-  size_t scratch;  // byte offset in the slot's grouped scratch
+  size_t scratch;  // byte offset in the batch's grouped scratch
 };
 
-int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
-  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
-  if (count && !jobs) return fail(AFRS_EINVAL, "jobs is NULL");
-  if (count > (size_t)1 << 24) return fail(AFRS_EINVAL, "too many jobs (%zu)", count);
+// One batch prepared on the host: which jobs run where, and the layout of
+// its device tables (descriptors of the generic persistent kernel, then one
+// descriptor array per shape group, then the task counter and the locator
+// table, which are written on the device).
+struct BatchPrep {
+  std::vector<size_t> valid;  // accepted jobs (status set to queued)
   std::vector<afrs::BatchJob> bj;
   std::vector<uint2> tasks;
   std::vector<int> rec;
   std::vector<uint8_t> pos;
   std::vector<GroupedJob> grouped;
-  std::vector<size_t> valid;
-  size_t grp_bytes = 0;
+  struct Group {
+    int op, n, t;
+    size_t first, count, desc_off, max_ncw;
+  };
+  std::vector<Group> groups;
+  size_t grp_bytes = 0;  // grouped scratch
   int max_rows = 0;
+  size_t o_jobs = 0, o_tasks = 0, o_rec = 0, o_pos = 0, o_cnt = 0, o_loc = 0;
+  size_t upload = 0;  // bytes the host writes
+  size_t total = 0;   // device table bytes
+  bool empty() const { return bj.empty() && grouped.empty(); }
+};
+
+// Validates the jobs (setting each one's status), groups them by shape and
+// lays out the tables.  Returns AFRS_OK or a negative code.
+int batch_prepare(afrs_job* jobs, size_t count, BatchPrep* p) {
   for (size_t i = 0; i < count; i++) {
     afrs_job& j = jobs[i];
     j.status = AFRS_EINVAL;
@@ -846,26 +863,26 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
       if (!j.src || !j.dst) continue;
     }
     j.status = enc ? 0 : 1;
-    valid.push_back(i);
+    p->valid.push_back(i);
   }
   // A shape group (encode: n, t; recover: n) runs on the specialised kernels
   // when it holds enough bytes to fill the GPU and its scratch fits the
-  // slot; the rest share one launch of the generic persistent kernel, which
-  // runs concurrently with the groups.
+  // grouped scratch; the rest share one launch of the generic persistent
+  // kernel, which runs concurrently with the groups.
   auto key = [&](const afrs_job& j) {
     return std::make_tuple((int)j.op, (int)j.n, j.op == AFRS_OP_ENCODE ? (int)j.t : 0);
   };
   std::map<std::tuple<int, int, int>, size_t> group_bytes;
-  for (size_t i : valid) group_bytes[key(jobs[i])] += (size_t)jobs[i].n * jobs[i].shard_len;
-  for (size_t i : valid) {
+  for (size_t i : p->valid) group_bytes[key(jobs[i])] += (size_t)jobs[i].n * jobs[i].shard_len;
+  for (size_t i : p->valid) {
     const afrs_job& j = jobs[i];
     const bool enc = j.op == AFRS_OP_ENCODE;
     const int op = enc ? 0 : 1;
     if (afrs::jobs_supported(op, (int)j.n, (int)j.t) && group_bytes[key(j)] >= kGroupMinBytes) {
       const size_t need = align256(afrs::job_scratch_bytes(op, (int)j.n, (int)j.t, j.shard_len));
-      if (grp_bytes + need <= kGroupScratchCap) {
-        grouped.push_back(GroupedJob{i, op, (int)j.n, std::get<2>(key(j)), grp_bytes});
-        grp_bytes += need;
+      if (p->grp_bytes + need <= kGroupScratchCap) {
+        p->grouped.push_back(GroupedJob{i, op, (int)j.n, std::get<2>(key(j)), p->grp_bytes});
+        p->grp_bytes += need;
         continue;
       }
     }
@@ -877,97 +894,62 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
     b.n = (int)j.n;
     b.t = (int)j.t;
     b.e = (int)j.e;
-    b.pos_off = (uint32_t)pos.size();
+    b.pos_off = (uint32_t)p->pos.size();
     if (!enc) {
-      b.loc = (uint32_t)rec.size();
-      rec.push_back((int)bj.size());
-      pos.insert(pos.end(), j.positions, j.positions + j.e);
-      max_rows = std::max(max_rows, 2 * (int)j.n);
+      b.loc = (uint32_t)p->rec.size();
+      p->rec.push_back((int)p->bj.size());
+      p->pos.insert(p->pos.end(), j.positions, j.positions + j.e);
+      p->max_rows = std::max(p->max_rows, 2 * (int)j.n);
     } else {
-      max_rows = std::max(max_rows, (int)j.t * ((int)(j.n / j.t) - 1 > 1 ? 2 : 1));
+      p->max_rows = std::max(p->max_rows, (int)j.t * ((int)(j.n / j.t) - 1 > 1 ? 2 : 1));
     }
     const size_t tiles = afrs::batch_tiles(j.shard_len);
-    for (size_t q = 0; q < tiles; q++) tasks.push_back(make_uint2((unsigned)bj.size(), (unsigned)q));
-    bj.push_back(b);
+    for (size_t q = 0; q < tiles; q++) p->tasks.push_back(make_uint2((unsigned)p->bj.size(), (unsigned)q));
+    p->bj.push_back(b);
   }
-  if (tasks.size() > (size_t)INT32_MAX) return fail(AFRS_EINVAL, "too many tiles");
-  if (bj.empty() && grouped.empty()) return AFRS_OK;
+  if (p->tasks.size() > (size_t)INT32_MAX) {
+    for (size_t i : p->valid) jobs[i].status = AFRS_EINVAL;
+    return fail(AFRS_EINVAL, "too many tiles");
+  }
   // Jobs sorted by shape (stable: caller order within a shape); the
   // descriptors of one shape group form one array.
-  std::stable_sort(grouped.begin(), grouped.end(), [](const GroupedJob& x, const GroupedJob& y) {
+  std::stable_sort(p->grouped.begin(), p->grouped.end(), [](const GroupedJob& x, const GroupedJob& y) {
     return std::make_tuple(x.op, x.n, x.t) < std::make_tuple(y.op, y.n, y.t);
   });
-  struct Group {
-    int op, n, t;
-    size_t first, count, desc_off, max_ncw;
-  };
-  std::vector<Group> groups;
-  const size_t o_jobs = 0;
-  const size_t o_tasks = align256(o_jobs + bj.size() * sizeof(afrs::BatchJob));
-  const size_t o_rec = align256(o_tasks + tasks.size() * sizeof(uint2));
-  const size_t o_pos = align256(o_rec + rec.size() * sizeof(int));
-  size_t o_grp = align256(o_pos + pos.size() + 1);
-  for (size_t q = 0; q < grouped.size(); q++) {
-    const GroupedJob& g = grouped[q];
+  p->o_jobs = 0;
+  p->o_tasks = align256(p->o_jobs + p->bj.size() * sizeof(afrs::BatchJob));
+  p->o_rec = align256(p->o_tasks + p->tasks.size() * sizeof(uint2));
+  p->o_pos = align256(p->o_rec + p->rec.size() * sizeof(int));
+  size_t o_grp = align256(p->o_pos + p->pos.size() + 1);
+  auto& groups = p->groups;
+  for (size_t q = 0; q < p->grouped.size(); q++) {
+    const GroupedJob& g = p->grouped[q];
     if (groups.empty() || groups.back().op != g.op || groups.back().n != g.n || groups.back().t != g.t) {
       if (!groups.empty()) o_grp = align256(o_grp + groups.back().count * afrs::job_desc_bytes(groups.back().op));
-      groups.push_back(Group{g.op, g.n, g.t, q, 0, o_grp, 0});
+      groups.push_back(BatchPrep::Group{g.op, g.n, g.t, q, 0, o_grp, 0});
     }
     groups.back().count++;
     groups.back().max_ncw = std::max(groups.back().max_ncw, afrs::job_colwords(jobs[g.job].shard_len));
   }
   if (!groups.empty()) o_grp = align256(o_grp + groups.back().count * afrs::job_desc_bytes(groups.back().op));
-  const size_t o_cnt = o_grp;
-  const size_t upload = o_cnt;  // the locator table and the counter are written on the device
-  const size_t o_loc = align256(o_cnt + sizeof(unsigned));
-  const size_t total = align256(o_loc + rec.size() * 768);
-  std::lock_guard<std::recursive_mutex> lk(c->mu);
-  DeviceGuard g(c->device);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // A failure before anything is enqueued leaves every accepted job unrun.
-  auto bail = [&](cudaError_t err, const char* what) -> int {
-    const int r = cuda_fail(err, what);
-    for (size_t i : valid) jobs[i].status = r;
-    return r;
-  };
-  const int slot = c->batch_slot;
-  c->batch_slot ^= 1;
-  // The slot's previous batch must be done with its staging, tables and scratch.
-  cudaError_t e = cudaEventSynchronize(c->batch_free[slot]);
-  if (e != cudaSuccess) return bail(e, "batch wait");
-  if (total > c->batch_dev_bytes[slot]) {
-    if (c->batch_dev[slot]) cudaFree(c->batch_dev[slot]);
-    c->batch_dev[slot] = nullptr;
-    c->batch_dev_bytes[slot] = 0;
-    if ((e = cudaMalloc(&c->batch_dev[slot], total * 2)) != cudaSuccess) return bail(e, "batch tables");
-    c->batch_dev_bytes[slot] = total * 2;
-  }
-  if (upload > c->batch_host_bytes[slot]) {
-    if (c->batch_host[slot]) cudaFreeHost(c->batch_host[slot]);
-    c->batch_host[slot] = nullptr;
-    c->batch_host_bytes[slot] = 0;
-    if ((e = cudaMallocHost(&c->batch_host[slot], upload * 2)) != cudaSuccess) return bail(e, "batch staging");
-    c->batch_host_bytes[slot] = upload * 2;
-  }
-  if (grp_bytes > c->grp_scratch_bytes[slot]) {
-    if (c->grp_scratch[slot]) cudaFree(c->grp_scratch[slot]);
-    c->grp_scratch[slot] = nullptr;
-    c->grp_scratch_bytes[slot] = 0;
-    const size_t want = std::min(kGroupScratchCap, grp_bytes * 2);
-    if ((e = cudaMalloc(reinterpret_cast<void**>(&c->grp_scratch[slot]), want)) != cudaSuccess)
-      return bail(e, "batch scratch");
-    c->grp_scratch_bytes[slot] = want;
-  }
-  uint8_t* h = c->batch_host[slot];
-  if (!bj.empty()) std::memcpy(h + o_jobs, bj.data(), bj.size() * sizeof(afrs::BatchJob));
-  if (!tasks.empty()) std::memcpy(h + o_tasks, tasks.data(), tasks.size() * sizeof(uint2));
-  if (!rec.empty()) std::memcpy(h + o_rec, rec.data(), rec.size() * sizeof(int));
-  if (!pos.empty()) std::memcpy(h + o_pos, pos.data(), pos.size());
-  uint8_t* scratch = reinterpret_cast<uint8_t*>(c->grp_scratch[slot]);
-  for (const Group& gr : groups) {
+  p->o_cnt = o_grp;
+  p->upload = p->o_cnt;  // the locator table and the counter are written on the device
+  p->o_loc = align256(p->o_cnt + sizeof(unsigned));
+  p->total = align256(p->o_loc + p->rec.size() * 768);
+  return AFRS_OK;
+}
+
+// Writes the batch's tables (host staging h, p.upload bytes) for grouped
+// scratch at device address `scratch`.
+void batch_fill(const BatchPrep& p, const afrs_job* jobs, uint8_t* h, uint8_t* scratch) {
+  if (!p.bj.empty()) std::memcpy(h + p.o_jobs, p.bj.data(), p.bj.size() * sizeof(afrs::BatchJob));
+  if (!p.tasks.empty()) std::memcpy(h + p.o_tasks, p.tasks.data(), p.tasks.size() * sizeof(uint2));
+  if (!p.rec.empty()) std::memcpy(h + p.o_rec, p.rec.data(), p.rec.size() * sizeof(int));
+  if (!p.pos.empty()) std::memcpy(h + p.o_pos, p.pos.data(), p.pos.size());
+  for (const BatchPrep::Group& gr : p.groups) {
     const size_t sz = afrs::job_desc_bytes(gr.op);
     for (size_t q = 0; q < gr.count; q++) {
-      const GroupedJob& gj = grouped[gr.first + q];
+      const GroupedJob& gj = p.grouped[gr.first + q];
       const afrs_job& j = jobs[gj.job];
       uint32_t* sc = reinterpret_cast<uint32_t*>(scratch + gj.scratch);
       void* desc = h + gr.desc_off + q * sz;
@@ -986,14 +968,129 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
       }
     }
   }
+}
+
+// Enqueues the kernels of a prepared batch whose tables are at `d` (device):
+// the group streams fork from `s`, the generic persistent kernel runs on
+// `s`, the shape groups (largest first) round-robin on the group streams,
+// and every forked stream is joined back into `s`, also after a failure.
+// Only kernel launches and event records: capturable in a CUDA graph.
+cudaError_t batch_enqueue(afrs_ctx* c, const BatchPrep& p, uint8_t* d, cudaStream_t s, const char** what) {
+  const int nstreams = (int)std::min<size_t>(4, p.groups.size());
+  int forked = 0;
+  cudaError_t e = cudaSuccess;
+  *what = "batch fork";
+  if (nstreams) e = cudaEventRecord(c->grp_fork, s);
+  for (int k = 0; k < nstreams && e == cudaSuccess; k++)
+    if ((e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_fork, 0)) == cudaSuccess) forked = k + 1;
+  if (e == cudaSuccess && !p.bj.empty()) {
+    afrs::BatchLaunch bl{};
+    bl.jobs = reinterpret_cast<const afrs::BatchJob*>(d + p.o_jobs);
+    bl.tasks = reinterpret_cast<const uint2*>(d + p.o_tasks);
+    bl.ntasks = (int)p.tasks.size();
+    bl.rec_jobs = reinterpret_cast<const int*>(d + p.o_rec);
+    bl.nrec = (int)p.rec.size();
+    bl.pos_tab = d + p.o_pos;
+    bl.loc_tab = d + p.o_loc;
+    bl.counter = reinterpret_cast<unsigned*>(d + p.o_cnt);
+    bl.max_rows = p.max_rows;
+    e = afrs::launch_batch(bl, s);
+    *what = "batch launch";
+  }
+  if (e == cudaSuccess) {
+    const auto& groups = p.groups;
+    std::vector<size_t> order(groups.size());
+    for (size_t q = 0; q < order.size(); q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+      return groups[x].count * groups[x].max_ncw * groups[x].n > groups[y].count * groups[y].max_ncw * groups[y].n;
+    });
+    for (size_t q = 0; q < order.size() && e == cudaSuccess; q++) {
+      const BatchPrep::Group& gr = groups[order[q]];
+      cudaStream_t gs = c->grp_stream[q % nstreams];
+      e = gr.op == 0 ? afrs::launch_encode_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs)
+                     : afrs::launch_recover_jobs(gr.n, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
+      *what = "batch group launch";
+    }
+  }
+  for (int k = 0; k < forked; k++) {
+    cudaError_t je = cudaEventRecord(c->grp_join[k], c->grp_stream[k]);
+    if (je == cudaSuccess) je = cudaStreamWaitEvent(s, c->grp_join[k], 0);
+    if (e == cudaSuccess && je != cudaSuccess) {
+      e = je;
+      *what = "batch join";
+    }
+  }
+  return e;
+}
+
+}  // namespace
+
+// A prepared batch (afrs_batch_plan_*): the tables and grouped scratch live
+// on the device for the plan's lifetime, so a launch enqueues kernels only.
+struct afrs_batch_plan {
+  afrs_ctx* ctx;
+  BatchPrep prep;
+  uint8_t* tables;   // prep.total bytes
+  uint8_t* scratch;  // prep.grp_bytes bytes
+};
+
+extern "C" {
+
+int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (count && !jobs) return fail(AFRS_EINVAL, "jobs is NULL");
+  if (count > (size_t)1 << 24) return fail(AFRS_EINVAL, "too many jobs (%zu)", count);
+  BatchPrep p;
+  int r = batch_prepare(jobs, count, &p);
+  if (r) return r;
+  if (p.empty()) return AFRS_OK;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  DeviceGuard g(c->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // A failure before anything is enqueued leaves every accepted job unrun.
+  auto bail = [&](cudaError_t err, const char* what) -> int {
+    const int rr = cuda_fail(err, what);
+    for (size_t i : p.valid) jobs[i].status = rr;
+    return rr;
+  };
+  const int slot = c->batch_slot;
+  c->batch_slot ^= 1;
+  // The slot's previous batch must be done with its staging, tables and scratch.
+  cudaError_t e = cudaEventSynchronize(c->batch_free[slot]);
+  if (e != cudaSuccess) return bail(e, "batch wait");
+  if (p.total > c->batch_dev_bytes[slot]) {
+    if (c->batch_dev[slot]) cudaFree(c->batch_dev[slot]);
+    c->batch_dev[slot] = nullptr;
+    c->batch_dev_bytes[slot] = 0;
+    if ((e = cudaMalloc(&c->batch_dev[slot], p.total * 2)) != cudaSuccess) return bail(e, "batch tables");
+    c->batch_dev_bytes[slot] = p.total * 2;
+  }
+  if (p.upload > c->batch_host_bytes[slot]) {
+    if (c->batch_host[slot]) cudaFreeHost(c->batch_host[slot]);
+    c->batch_host[slot] = nullptr;
+    c->batch_host_bytes[slot] = 0;
+    if ((e = cudaMallocHost(&c->batch_host[slot], p.upload * 2)) != cudaSuccess) return bail(e, "batch staging");
+    c->batch_host_bytes[slot] = p.upload * 2;
+  }
+  if (p.grp_bytes > c->grp_scratch_bytes[slot]) {
+    if (c->grp_scratch[slot]) cudaFree(c->grp_scratch[slot]);
+    c->grp_scratch[slot] = nullptr;
+    c->grp_scratch_bytes[slot] = 0;
+    const size_t want = std::min(kGroupScratchCap, p.grp_bytes * 2);
+    if ((e = cudaMalloc(reinterpret_cast<void**>(&c->grp_scratch[slot]), want)) != cudaSuccess)
+      return bail(e, "batch scratch");
+    c->grp_scratch_bytes[slot] = want;
+  }
+  uint8_t* h = c->batch_host[slot];
+  batch_fill(p, jobs, h, reinterpret_cast<uint8_t*>(c->grp_scratch[slot]));
   uint8_t* d = c->batch_dev[slot];
   // Every exit from here on records batch_free[slot] on `s` (the next call on
   // this slot waits for it before it rewrites the slot's staging and
-  // tables), joins every group stream it forked, and on failure marks the
-  // jobs as not run.
+  // tables) and on failure marks the jobs as not run; batch_enqueue joins
+  // every group stream it forked.
   auto finish = [&](cudaError_t err, const char* what) -> int {
     if (err != cudaSuccess)
-      for (size_t i : valid) jobs[i].status = AFRS_ECUDA;
+      for (size_t i : p.valid) jobs[i].status = AFRS_ECUDA;
     cudaError_t re = cudaEventRecord(c->batch_free[slot], s);
     if (err == cudaSuccess && re != cudaSuccess) {
       err = re;
@@ -1001,56 +1098,76 @@ int afrs_batch_dev(afrs_ctx* c, afrs_job* jobs, size_t count, void* stream) {
     }
     return err == cudaSuccess ? AFRS_OK : cuda_fail(err, what);
   };
-  if ((e = cudaMemcpyAsync(d, h, upload, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+  if ((e = cudaMemcpyAsync(d, h, p.upload, cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return finish(e, "batch upload");
-  // Fork the group streams right after the upload, so that the groups run
-  // concurrently with the generic kernel below.
-  const int nstreams = (int)std::min<size_t>(4, groups.size());
-  int forked = 0;
-  const char* what = "batch fork";
-  if (nstreams) e = cudaEventRecord(c->grp_fork, s);
-  for (int k = 0; k < nstreams && e == cudaSuccess; k++)
-    if ((e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_fork, 0)) == cudaSuccess) forked = k + 1;
-  if (e == cudaSuccess && !bj.empty()) {
-    afrs::BatchLaunch bl{};
-    bl.jobs = reinterpret_cast<const afrs::BatchJob*>(d + o_jobs);
-    bl.tasks = reinterpret_cast<const uint2*>(d + o_tasks);
-    bl.ntasks = (int)tasks.size();
-    bl.rec_jobs = reinterpret_cast<const int*>(d + o_rec);
-    bl.nrec = (int)rec.size();
-    bl.pos_tab = d + o_pos;
-    bl.loc_tab = d + o_loc;
-    bl.counter = reinterpret_cast<unsigned*>(d + o_cnt);
-    bl.max_rows = max_rows;
-    e = afrs::launch_batch(bl, s);
-    what = "batch launch";
-  }
-  // Shape groups are independent: largest first, round-robin over the group
-  // streams, after the upload, joined back into `s`.
-  if (e == cudaSuccess) {
-    std::vector<size_t> order(groups.size());
-    for (size_t q = 0; q < order.size(); q++) order[q] = q;
-    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
-      return groups[x].count * groups[x].max_ncw * groups[x].n > groups[y].count * groups[y].max_ncw * groups[y].n;
-    });
-    for (size_t q = 0; q < order.size() && e == cudaSuccess; q++) {
-      const Group& gr = groups[order[q]];
-      cudaStream_t gs = c->grp_stream[q % nstreams];
-      e = gr.op == 0 ? afrs::launch_encode_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs)
-                     : afrs::launch_recover_jobs(gr.n, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
-      what = "batch group launch";
-    }
-  }
-  // Join every forked stream, also after a failed launch.
-  for (int k = 0; k < forked; k++) {
-    cudaError_t je = cudaEventRecord(c->grp_join[k], c->grp_stream[k]);
-    if (je == cudaSuccess) je = cudaStreamWaitEvent(s, c->grp_join[k], 0);
-    if (e == cudaSuccess && je != cudaSuccess) {
-      e = je;
-      what = "batch join";
-    }
-  }
+  const char* what = "";
+  e = batch_enqueue(c, p, d, s, &what);
   return finish(e, what);
+}
+
+int afrs_batch_plan_create(afrs_ctx* c, afrs_job* jobs, size_t count, afrs_batch_plan** out) {
+  if (!out) return fail(AFRS_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
+  if (count && !jobs) return fail(AFRS_EINVAL, "jobs is NULL");
+  if (count > (size_t)1 << 24) return fail(AFRS_EINVAL, "too many jobs (%zu)", count);
+  afrs_batch_plan* pl = new (std::nothrow) afrs_batch_plan{};
+  if (!pl) return fail(AFRS_ENOMEM, "plan allocation");
+  pl->ctx = c;
+  int r = batch_prepare(jobs, count, &pl->prep);
+  if (r) {
+    delete pl;
+    return r;
+  }
+  if (!pl->prep.empty()) {
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    const BatchPrep& p = pl->prep;
+    cudaError_t e = cudaMalloc(&pl->tables, p.total);
+    const char* what = "plan tables";
+    if (e == cudaSuccess && p.grp_bytes) {
+      e = cudaMalloc(&pl->scratch, p.grp_bytes);
+      what = "plan scratch";
+    }
+    if (e == cudaSuccess) {
+      std::vector<uint8_t> h(p.upload);
+      batch_fill(p, jobs, h.data(), pl->scratch);
+      e = cudaMemcpy(pl->tables, h.data(), p.upload, cudaMemcpyHostToDevice);
+      what = "plan upload";
+    }
+    if (e != cudaSuccess) {
+      r = cuda_fail(e, what);
+      for (size_t i : p.valid) jobs[i].status = r;
+      if (pl->tables) cudaFree(pl->tables);
+      if (pl->scratch) cudaFree(pl->scratch);
+      delete pl;
+      return r;
+    }
+  }
+  *out = pl;
+  return AFRS_OK;
+}
+
+int afrs_batch_plan_launch(afrs_batch_plan* pl, void* stream) {
+  if (!pl) return fail(AFRS_EINVAL, "plan is NULL");
+  if (pl->prep.empty()) return AFRS_OK;
+  afrs_ctx* c = pl->ctx;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  DeviceGuard g(c->device);
+  const char* what = "";
+  cudaError_t e = batch_enqueue(c, pl->prep, pl->tables, static_cast<cudaStream_t>(stream), &what);
+  return e == cudaSuccess ? AFRS_OK : cuda_fail(e, what);
+}
+
+void afrs_batch_plan_destroy(afrs_batch_plan* pl) {
+  if (!pl) return;
+  if (pl->tables || pl->scratch) {
+    DeviceGuard g(pl->ctx->device);
+    cudaDeviceSynchronize();  // no launch of the plan may still read its tables
+    if (pl->tables) cudaFree(pl->tables);
+    if (pl->scratch) cudaFree(pl->scratch);
+  }
+  delete pl;
 }
 
 }  // extern "C"

@@ -131,6 +131,22 @@ typedef struct afrs_job {
 } afrs_job;
 int afrs_batch_dev(afrs_ctx* ctx, afrs_job* jobs, size_t count, void* stream);
 
+/* A batch prepared once and launched many times (no counterpart in the
+ * reference).  afrs_batch_plan_create validates the jobs as afrs_batch_dev
+ * does (setting each job's status), groups them by shape and copies their
+ * descriptor tables to device memory owned by the plan, synchronously; the
+ * jobs' buffers are the ones the plan runs on, every launch.
+ * afrs_batch_plan_launch enqueues the plan's kernels on `stream` (the group
+ * streams of the plan's context fork from it and join back), with no host
+ * work and no copy, so the launch can be captured into a CUDA graph and the
+ * graph replayed.  Launches of one plan share its tables and scratch and
+ * must not overlap on the GPU; the context must outlive its plans.
+ * afrs_batch_plan_destroy waits for the device and frees the plan. */
+typedef struct afrs_batch_plan afrs_batch_plan;
+int afrs_batch_plan_create(afrs_ctx* ctx, afrs_job* jobs, size_t count, afrs_batch_plan** out);
+int afrs_batch_plan_launch(afrs_batch_plan* plan, void* stream);
+void afrs_batch_plan_destroy(afrs_batch_plan* plan);
+
 /* Allocation-free erasure recovery.  No counterpart in the reference: it
  * exists for callers that cannot allocate device memory when they recover,
  * e.g. code inside CUDA stream capture (cudaMalloc is not allowed there),
