@@ -67,8 +67,9 @@ SIGNATURES = {
 
 
 def build(jobs: int = 8) -> str:
-    """Compile csrc/ with nvcc for sm_100a; returns the library path."""
-    subprocess.run(["make", "-s", f"-j{jobs}", "-C", os.path.join(HERE, "csrc")], check=True)
+    """Compile csrc/ with nvcc for sm_100a (the library and the multiply
+    benchmark program); returns the library path."""
+    subprocess.run(["make", "-s", f"-j{jobs}", "-C", os.path.join(HERE, "csrc"), "all", "bench_multiply"], check=True)
     return LIB_PATH
 
 
