@@ -19,6 +19,10 @@ _u8p = ctypes.c_void_p
 _sz = ctypes.c_size_t
 _u32 = ctypes.c_uint32
 
+AFRS_HOST_AUTO = 0
+AFRS_HOST_STAGED = 1
+AFRS_HOST_DIRECT = 2
+
 AFRS_ROUTE_TABLE = 0
 AFRS_ROUTE_GENERIC = 1
 AFRS_ROUTE_SPECIAL = 2

@@ -217,6 +217,8 @@ def main():
     ap.add_argument("--e2e-pairs", type=int, default=3, help="host thread pairs (encode + recover) of the e2e line")
     ap.add_argument("--workload", default="codeword", choices=["codeword", "small", "batched", "serving", "large", "kernels"])
     ap.add_argument("--shard-len", type=int, default=0, help="--workload large: shard length (default 4 MiB)")
+    ap.add_argument("--host-mode", default="auto", choices=["auto", "staged", "direct"],
+                    help="how the e2e line's host-buffer calls move data (afrs_ctx_set_staging)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -466,6 +468,11 @@ def main():
                   (afrs.Codec(n, t, device=local, context=afrs.Context(local)),
                    afrs.Codec(n, t, device=local, context=afrs.Context(local))) for i in range(P)]
     e2e_steps = max(3, min(args.steps, 150))
+    mode = {"auto": afrs._lib.AFRS_HOST_AUTO, "staged": afrs._lib.AFRS_HOST_STAGED,
+            "direct": afrs._lib.AFRS_HOST_DIRECT}[args.host_mode]
+    for pair in e2e_codecs:
+        for cdc in pair:
+            afrs.codec._check(afrs.lib().afrs_ctx_set_staging(cdc.ctx.handle, 0, 0, mode), "afrs_ctx_set_staging")
 
     def e2e_encode(i):
         e2e_codecs[i][0].encode_parity(h_msg, h_pars[i], L)
@@ -544,8 +551,8 @@ def main():
         "e2e": {"value": round(e2e_value, 3), "unit": "GB/s",
                 "h2d_bytes_per_step": int(h2d_step), "d2h_bytes_per_step": int(d2h_step),
                 "steps": e2e_total,
-                "how": (f"host-buffer API, page-locked buffers; {P} pairs of host threads (encode, recover), "
-                        "own contexts and codewords, steps back to back; wall time") if overlap
+                "how": (f"host-buffer API, page-locked buffers, staging {args.host_mode}; {P} pairs of host threads "
+                        "(encode, recover), own contexts and codewords, steps back to back; wall time") if overlap
                        else "host-buffer API, page-locked buffers; encode then recover per step, one thread"},
         "gpu_launches": int(launches),
         "timed_regions": {"count": len(region_ms), "median_ms": round(statistics.median(region_ms), 5),
