@@ -217,6 +217,10 @@ def main():
     ap.add_argument("--e2e-pairs", type=int, default=3, help="host thread pairs (encode + recover) of the e2e line")
     ap.add_argument("--workload", default="codeword", choices=["codeword", "small", "batched", "serving", "large", "kernels"])
     ap.add_argument("--shard-len", type=int, default=0, help="--workload large: shard length (default 4 MiB)")
+    ap.add_argument("--priority", default="none", choices=["none", "recover", "encode"],
+                    help="give this operation's streams the higher CUDA stream priority")
+    ap.add_argument("--work-cap", type=int, default=0,
+                    help="scratch cap (bytes) of the device-path contexts (afrs_ctx_set_work_cap; 0 = default)")
     ap.add_argument("--host-mode", default="auto", choices=["auto", "staged", "direct"],
                     help="how the e2e line's host-buffer calls move data (afrs_ctx_set_staging)")
     args = ap.parse_args()
@@ -280,8 +284,13 @@ def main():
     assert R % S == 0, "--pairs must divide the number of rotating codewords"
     codec_e = [afrs.Codec(n, t, device=local, context=afrs.Context(local)) for _ in range(S)]
     codec_r = [afrs.Codec(n, t, device=local, context=afrs.Context(local)) for _ in range(S)]
-    s_enc = [torch.cuda.Stream(dev) if overlap else stream for _ in range(S)]
-    s_rec = [torch.cuda.Stream(dev) if overlap else stream for _ in range(S)]
+    if args.work_cap:
+        for cdc in codec_e + codec_r:
+            cdc.ctx.set_work_cap(args.work_cap)
+    pe = -1 if args.priority == "encode" else 0
+    pr = -1 if args.priority == "recover" else 0
+    s_enc = [torch.cuda.Stream(dev, priority=pe) if overlap else stream for _ in range(S)]
+    s_rec = [torch.cuda.Stream(dev, priority=pr) if overlap else stream for _ in range(S)]
 
     def enc_call(r):
         m, p = enc_bufs[r]
@@ -533,6 +542,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": n, "k": k, "t": t, "shard_len": L, "erasures": t,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "work_cap": args.work_cap or None,
+                   "stream_priority": args.priority,
                    "overlap": (f"encode and recover of a step on two streams; steps round-robin over {S} "
                                "stream pairs (own contexts)") if overlap else "encode then recover on one stream",
                    "launch": ("one CUDA graph per rotation of the codewords (all streams), replayed"
