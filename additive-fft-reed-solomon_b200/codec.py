@@ -21,6 +21,7 @@ stream and returns without waiting).  Where the reference panics (bad sizes,
 from __future__ import annotations
 
 import ctypes
+import struct
 
 import numpy as np
 
@@ -246,17 +247,39 @@ class Job:
         return self.n * self.shard_len
 
 
+# struct afrs_job of include/afrs.h: op, n, t, e (u32), shard_len, src, dst
+# (64-bit) = 40 bytes, then positions[256], status (i32), reserved (u32).
+_JOB_HEAD = struct.Struct("<IIIIQQQ")
+_JOB_TAIL = 256 + 8
+_JOB_STATUS = 296 // 4  # int32 index of status within a record
+_JOB_WORDS = 304 // 4
+
+
+def _job_record(j) -> bytes:
+    """The 304 bytes of ``j`` as a struct afrs_job."""
+    try:
+        pos = bytes(j.positions[:256])
+    except ValueError:
+        raise AfrsError(_lib.AFRS_EINVAL, "erasure positions must fit in u8") from None
+    src = _dev_ptr(j.src) if j.src is not None else 0
+    dst = _dev_ptr(j.dst) if j.dst is not None else 0
+    return _JOB_HEAD.pack(j.op, j.n, j.t, len(j.positions), j.shard_len, src, dst) + pos + bytes(_JOB_TAIL - len(pos))
+
+
 def _job_array(jobs):
-    arr = (_lib.AfrsJob * max(len(jobs), 1))()
-    for i, j in enumerate(jobs):
-        a = arr[i]
-        a.op, a.n, a.t, a.shard_len = j.op, j.n, j.t, j.shard_len
-        a.e = len(j.positions)
-        for q, p in enumerate(j.positions[:256]):
-            a.positions[q] = p
-        a.src = _dev_ptr(j.src) if j.src is not None else None
-        a.dst = _dev_ptr(j.dst) if j.dst is not None else None
-    return arr
+    """ctypes array of struct afrs_job for ``jobs``: one record packed per job
+    and one copy into the array (a few microseconds per job less than setting
+    the ctypes fields one by one, which matters when a server packs hundreds
+    of requests per batch)."""
+    n = max(len(jobs), 1)
+    buf = b"".join(_job_record(j) for j in jobs) if jobs else bytes(ctypes.sizeof(_lib.AfrsJob))
+    return (_lib.AfrsJob * n).from_buffer_copy(buf)
+
+
+def _job_statuses(arr, count: int) -> list:
+    """The status fields of the first ``count`` records of a job array."""
+    words = np.frombuffer(arr, dtype=np.int32)
+    return words[_JOB_STATUS:count * _JOB_WORDS:_JOB_WORDS].tolist()
 
 
 def run_batch(jobs, device: int = 0, stream=None) -> list:
@@ -268,10 +291,9 @@ def run_batch(jobs, device: int = 0, stream=None) -> list:
     ctx = Context.get(device)
     s = stream if stream is not None else torch.cuda.current_stream(device)
     _check(_lib.lib().afrs_batch_dev(ctx.handle, arr, len(jobs), s.cuda_stream), "afrs_batch_dev")
-    out = []
-    for i, j in enumerate(jobs):
-        j.status = int(arr[i].status)
-        out.append(j.status)
+    out = _job_statuses(arr, len(jobs))
+    for j, st in zip(jobs, out):
+        j.status = st
     return out
 
 
@@ -289,10 +311,9 @@ class BatchPlan:
         self._h = ctypes.c_void_p()
         _check(_lib.lib().afrs_batch_plan_create(self.ctx.handle, arr, len(self.jobs), ctypes.byref(self._h)),
                "afrs_batch_plan_create")
-        self.statuses = []
-        for i, j in enumerate(self.jobs):
-            j.status = int(arr[i].status)
-            self.statuses.append(j.status)
+        self.statuses = _job_statuses(arr, len(self.jobs))
+        for j, st in zip(self.jobs, self.statuses):
+            j.status = st
 
     def launch(self, stream=None) -> None:
         import torch

@@ -12,21 +12,25 @@ serves the same requests one call at a time (the per-call path).
 Both record, per request, the latency from arrival to completion (host
 clock, completion observed through CUDA events).
 
-Stream order: ``submit`` records an event on the caller's current stream, and
-the stream that runs the request waits on it, so work the caller enqueued on
-the request's buffers before submitting (a fill, a copy) is finished first.
-The buffers are also recorded on the running stream, so that torch's caching
-allocator does not hand their memory to another tensor while the request is
-still on the GPU.
+Stream order: ``submit`` / ``submit_many`` record one event on the caller's
+current stream for the requests they accept, and the stream that runs a
+request waits on it, so work the caller enqueued on the request's buffers
+before submitting (a fill, a copy) is finished first.  The buffers are also
+recorded on the running stream, so that torch's caching allocator does not
+hand their memory to another tensor while the request is still on the GPU.
+
+Host cost per request is what bounds a server of small requests, so events
+are reused (creating a CUDA event costs several microseconds, recording a
+reused one about one), requests that arrive together share one submission
+event, and a batch's stream waits once per distinct submission event.
 """
 from __future__ import annotations
 
 import collections
-import ctypes
 import time
 
 from . import _lib
-from .codec import Codec, Context, Job, _check, _dev_ptr
+from .codec import Codec, Context, Job, _check, _job_array, _job_statuses
 
 __all__ = ["Request", "BatchServer", "PlainServer", "percentiles", "make_job_array"]
 
@@ -40,19 +44,31 @@ class Request(Job):
         self.done = None
         self.ready = None  # event on the submitter's stream (mark_submitted)
 
-    def mark_submitted(self) -> None:
+    def mark_submitted(self, event=None) -> None:
         """Records, on the caller's current stream, the point after which the
-        request's buffers may be used."""
+        request's buffers may be used (or takes ``event``, recorded there
+        already, which requests submitted together share)."""
         import torch
 
-        self.ready = torch.cuda.Event()
-        self.ready.record()
+        if event is None:
+            event = torch.cuda.Event()
+            event.record()
+        self.ready = event
 
-    def enter_stream(self, s) -> None:
+    def enter_stream(self, s, events=None, waited=None) -> None:
         """Orders stream ``s`` after the submitter's work on the buffers and
-        keeps the buffers' memory from being reused before ``s`` is done."""
-        if self.ready is not None:
-            s.wait_event(self.ready)
+        keeps the buffers' memory from being reused before ``s`` is done.
+        ``waited`` (a set) holds the ids of submission events ``s`` already
+        waits on; ``events`` (an _EventPool) takes the event back once every
+        request sharing it has entered its stream."""
+        ev = self.ready
+        if ev is not None:
+            if waited is None or id(ev) not in waited:
+                s.wait_event(ev)
+                if waited is not None:
+                    waited.add(id(ev))
+            if events is not None:
+                events.release(ev)
         for buf in (self.src, self.dst):
             if buf is not None and hasattr(buf, "record_stream"):
                 buf.record_stream(s)
@@ -62,18 +78,41 @@ class Request(Job):
         return self.done - self.arrival
 
 
+class _EventPool:
+    """CUDA events for reuse.  ``record`` hands out a recorded event that
+    ``uses`` holders will ``release``; after the last release it is recorded
+    again for a later holder.  Re-recording is safe once the holders are done
+    with it: a stream wait enqueued on an event keeps the work the event
+    captured when the wait was enqueued, and completion events are released
+    only after ``query()`` returned True."""
+
+    def __init__(self):
+        self.free = []
+        self.uses = {}
+
+    def record(self, stream=None, uses: int = 1):
+        import torch
+
+        ev = self.free.pop() if self.free else torch.cuda.Event()
+        ev.record(stream)
+        self.uses[id(ev)] = (ev, uses)
+        return ev
+
+    def release(self, ev) -> None:
+        k = id(ev)
+        held = self.uses.get(k)
+        if held is None:
+            return
+        if held[1] <= 1:
+            del self.uses[k]
+            self.free.append(ev)
+        else:
+            self.uses[k] = (ev, held[1] - 1)
+
+
 def make_job_array(jobs):
     """ctypes array of struct afrs_job for ``jobs`` (see include/afrs.h)."""
-    arr = (_lib.AfrsJob * max(len(jobs), 1))()
-    for i, j in enumerate(jobs):
-        a = arr[i]
-        a.op, a.n, a.t, a.shard_len = j.op, j.n, j.t, j.shard_len
-        a.e = len(j.positions)
-        for q, p in enumerate(j.positions[:256]):
-            a.positions[q] = p
-        a.src = _dev_ptr(j.src) if j.src is not None else None
-        a.dst = _dev_ptr(j.dst) if j.dst is not None else None
-    return arr
+    return _job_array(jobs)
 
 
 def percentiles(values, ps=(50, 99, 99.9)):
@@ -112,14 +151,25 @@ class BatchServer:
         self.inflight_bytes = 0
         self.batches = 0
         self.large_bytes = large_bytes
-        self.large = PlainServer(device, window=4)
+        self.events = _EventPool()
+        # Large requests queue on the GPU up to 16 deep, so that their stream
+        # keeps running while the host packs the next batch of small ones.
+        self.large = PlainServer(device, window=16, events=self.events)
 
     def submit(self, req: Request) -> None:
-        req.mark_submitted()
-        if req.nbytes >= self.large_bytes:
-            self.large.submit(req)
-        else:
-            self.queue.append(req)
+        self.submit_many((req,))
+
+    def submit_many(self, reqs) -> None:
+        """Accepts requests that arrived together (one submission event)."""
+        if not reqs:
+            return
+        ev = self.events.record(uses=len(reqs))
+        for r in reqs:
+            r.mark_submitted(ev)
+            if r.nbytes >= self.large_bytes:
+                self.large.queue.append(r)
+            else:
+                self.queue.append(r)
 
     def pending(self) -> int:
         return len(self.queue) + sum(len(b[1]) for b in self.busy if b is not None) + self.large.pending()
@@ -142,8 +192,6 @@ class BatchServer:
 
     def poll(self) -> list:
         """Retire finished batches, launch new ones; returns finished requests."""
-        import torch
-
         finished = self._poll_large()
         now = time.perf_counter()
         for i, b in enumerate(self.busy):
@@ -152,6 +200,7 @@ class BatchServer:
                     r.done = now
                 finished.extend(b[1])
                 self.inflight_bytes -= b[2]
+                self.events.release(b[0])
                 self.busy[i] = None
         for i in range(len(self.streams)):
             if self.busy[i] is not None or not self.queue:
@@ -169,14 +218,13 @@ class BatchServer:
                 break
             arr = make_job_array(take)
             s = self.streams[i]
+            waited = set()
             for r in take:
-                r.enter_stream(s)
+                r.enter_stream(s, self.events, waited)
             _check(_lib.lib().afrs_batch_dev(self.ctx.handle, arr, len(take), s.cuda_stream), "afrs_batch_dev")
-            for q, r in enumerate(take):
-                r.status = int(arr[q].status)
-            ev = torch.cuda.Event()
-            ev.record(s)
-            self.busy[i] = (ev, take, nbytes)
+            for r, st in zip(take, _job_statuses(arr, len(take))):
+                r.status = st
+            self.busy[i] = (self.events.record(s), take, nbytes)
             self.inflight_bytes += nbytes
             self.batches += 1
         return finished
@@ -185,7 +233,7 @@ class BatchServer:
 class PlainServer:
     """One request per call, in arrival order, on one stream."""
 
-    def __init__(self, device: int = 0, window: int = 64):
+    def __init__(self, device: int = 0, window: int = 64, events: "_EventPool | None" = None):
         import torch
 
         self.device = device
@@ -194,11 +242,19 @@ class PlainServer:
         self.inflight = collections.deque()  # (event, request)
         self.window = window
         self.codecs = {}
+        self.events = events if events is not None else _EventPool()
 
     def submit(self, req: Request) -> None:
-        if req.ready is None:
-            req.mark_submitted()
-        self.queue.append(req)
+        self.submit_many((req,))
+
+    def submit_many(self, reqs) -> None:
+        """Accepts requests that arrived together (one submission event)."""
+        if not reqs:
+            return
+        ev = self.events.record(uses=len(reqs))
+        for r in reqs:
+            r.mark_submitted(ev)
+            self.queue.append(r)
 
     def pending(self) -> int:
         return len(self.queue) + len(self.inflight)
@@ -215,22 +271,24 @@ class PlainServer:
         finished = []
         now = time.perf_counter()
         while self.inflight and self.inflight[0][0].query():
-            _, r = self.inflight.popleft()
+            ev, r = self.inflight.popleft()
             r.done = now
+            self.events.release(ev)
             finished.append(r)
+        if not self.queue or len(self.inflight) >= self.window:
+            return finished
+        waited = set()
         with torch.cuda.stream(self.stream):
             while self.queue and len(self.inflight) < self.window:
                 r = self.queue.popleft()
-                r.enter_stream(self.stream)
+                r.enter_stream(self.stream, self.events, waited)
                 c = self._codec(r.n, r.t)
                 if r.op == _lib.AFRS_OP_ENCODE:
                     c.encode_parity(r.src, r.dst, r.shard_len)
                     r.status = 0
                 else:
                     r.status = int(c.recover_erasure_shards(r.dst, None, r.shard_len, r.positions))
-                ev = torch.cuda.Event()
-                ev.record(self.stream)
-                self.inflight.append((ev, r))
+                self.inflight.append((self.events.record(self.stream), r))
         return finished
 
 
@@ -245,10 +303,13 @@ def serve_open_loop(server, requests, arrivals, timeout_s: float = 60.0):
         now = time.perf_counter()
         if now - t0 > timeout_s:
             raise TimeoutError(f"serving did not finish in {timeout_s} s ({len(done)}/{n} done)")
+        due = []
         while i < n and t0 + arrivals[i] <= now:
             requests[i].arrival = t0 + arrivals[i]
-            server.submit(requests[i])
+            due.append(requests[i])
             i += 1
+        if due:
+            server.submit_many(due)
         done.extend(server.poll())
         if i < n and not server.pending():
             time.sleep(max(0.0, min(1e-4, t0 + arrivals[i] - time.perf_counter())))

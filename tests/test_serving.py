@@ -96,3 +96,71 @@ def test_admission_cap_and_plain_server(afrs):
     for r, p, want in zip(reqs, preqs, expect):
         assert (r.dst.cpu().numpy() == want).all()
         assert torch.equal(r.dst, p.dst)
+
+
+class _FakeEvent:
+    def __init__(self):
+        self.records = 0
+
+    def record(self, stream=None):
+        self.records += 1
+
+
+def test_event_pool_reuses_an_event_after_its_last_holder(afrs):
+    pool = afrs.serving._EventPool()
+    a, b = _FakeEvent(), _FakeEvent()
+    pool.free = [b, a]
+    ev = pool.record(uses=3)
+    assert ev is a and a.records == 1
+    pool.release(ev)
+    pool.release(ev)
+    assert pool.free == [b]  # two of three holders released it
+    pool.release(ev)
+    assert pool.free == [b, a]
+    pool.release(ev)  # not held any more: ignored
+    assert pool.free == [b, a]
+    assert pool.record() is a and a.records == 2
+    pool.release(_FakeEvent())  # an event the pool never handed out
+    assert pool.free == [b]
+
+
+def test_a_batch_stream_waits_once_per_submission_event(afrs):
+    S = afrs.serving
+
+    class Stream:
+        def __init__(self):
+            self.waits = []
+
+        def wait_event(self, ev):
+            self.waits.append(ev)
+
+    pool = S._EventPool()
+    e1, e2 = _FakeEvent(), _FakeEvent()
+    pool.free = [e2, e1]
+    reqs = [S.Request(afrs.Job(1, 32, 8, None, None, 64, [1])) for _ in range(5)]
+    first = pool.record(uses=3)
+    second = pool.record(uses=2)
+    for r in reqs[:3]:
+        r.mark_submitted(first)
+    for r in reqs[3:]:
+        r.mark_submitted(second)
+    s, waited = Stream(), set()
+    for r in reqs:
+        r.enter_stream(s, pool, waited)
+    assert s.waits == [first, second]
+    assert sorted(map(id, pool.free)) == sorted([id(e1), id(e2)]) and not pool.uses
+
+
+def test_job_array_layout(afrs):
+    """The packed records match struct afrs_job field by field."""
+    jobs = [afrs.Job(1, 128, 32, None, None, 1024, [3, 5, 200]), afrs.Job(0, 64, 8, None, None, 64)]
+    arr = afrs.codec._job_array(jobs)
+    a, b = arr[0], arr[1]
+    assert (a.op, a.n, a.t, a.e, a.shard_len, a.status) == (1, 128, 32, 3, 1024, 0)
+    assert list(a.positions[:4]) == [3, 5, 200, 0] and not a.src and not a.dst
+    assert (b.op, b.n, b.t, b.e, b.shard_len) == (0, 64, 8, 0, 64) and not any(b.positions)
+    a.status, b.status = 7, -3
+    assert afrs.codec._job_statuses(arr, 2) == [7, -3]
+    with pytest.raises(afrs.AfrsError):
+        afrs.codec._job_array([afrs.Job(1, 128, 32, None, None, 1024, [300])])
+    assert len(afrs.codec._job_array([])) == 1
