@@ -221,12 +221,13 @@ def run_serving(args):
     # warm up both paths and every kernel shape in the pool
     run(S.BatchServer, build(200), [0.0] * 200)
     run(S.PlainServer, build(200), [0.0] * 200)
-    cap_reqs = build(600)
-    cap_b = run(S.BatchServer, cap_reqs, [0.0] * len(cap_reqs))
-    cap_p = run(S.PlainServer, build(600), [0.0] * 600)
+    # Capacity = the best of three closed-loop runs of 600 requests (all
+    # arriving at once): single runs vary with what the first ones warm up.
+    cap_b = max((run(S.BatchServer, build(600), [0.0] * 600) for _ in range(3)), key=lambda r: r["GB/s"])
+    cap_p = max((run(S.PlainServer, build(600), [0.0] * 600) for _ in range(3)), key=lambda r: r["GB/s"])
     mean_bytes = sum(j.nbytes for j in pool) / len(pool)
     levels = []
-    for frac in (0.1, 0.25, 0.5, 0.75, 1.0, 1.2):
+    for frac in (0.1, 0.25, 0.5, 0.75, 0.9, 1.0, 1.2):
         rate = frac * cap_b["GB/s"] * 1e9 / mean_bytes  # requests per second
         count = int(min(1500, max(100, rate * 0.6)))
         arrivals = np.cumsum(rng.exponential(1.0 / rate, count)).tolist()
@@ -234,23 +235,31 @@ def run_serving(args):
         row["batched"] = run(S.BatchServer, build(count), arrivals)
         row["per_call"] = run(S.PlainServer, build(count), arrivals)
         levels.append(row)
-    # Equal-p99 comparison: the per-call server's highest delivered
-    # throughput whose p99 is no worse than the batched server's at 100 % of
-    # the batched capacity, from a finer sweep of the per-call offered load.
-    target = next(r for r in levels if r["offered_frac_of_batched_capacity"] == 1.0)["batched"]
+    # Equal-p99 comparison: for every load level of the batched server, the
+    # per-call server's highest delivered throughput whose p99 is no worse,
+    # from a finer sweep of the per-call offered load (plus the per-call runs
+    # of the levels above).  The ratio depends on the p99 compared at, so
+    # every level is reported.
     sweep = []
-    for frac in (0.02, 0.05, 0.1, 0.15, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9):
+    for frac in (0.02, 0.05, 0.1, 0.15, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0):
         rate = frac * cap_p["GB/s"] * 1e9 / mean_bytes
         count = int(min(1500, max(100, rate * 0.6)))
         arrivals = np.cumsum(rng.exponential(1.0 / rate, count)).tolist()
         res = run(S.PlainServer, build(count), arrivals)
         res["offered_frac_of_per_call_capacity"] = frac
         sweep.append(res)
-    ok = [r for r in sweep if r["p99_ms"] <= target["p99_ms"]]
-    best = max(ok, key=lambda r: r["GB/s"]) if ok else None
-    iso = {"batched_at_full_load": target, "per_call_sweep": sweep,
-           "per_call_best_at_equal_or_lower_p99": best,
-           "throughput_ratio": round(target["GB/s"] / best["GB/s"], 2) if best else None}
+    per_call_points = sweep + [r["per_call"] for r in levels]
+    curve = []
+    for r in levels:
+        b = r["batched"]
+        ok = [p for p in per_call_points if p["p99_ms"] <= b["p99_ms"]]
+        best = max(ok, key=lambda p: p["GB/s"]) if ok else None
+        curve.append({"offered_frac_of_batched_capacity": r["offered_frac_of_batched_capacity"],
+                      "batched_p99_ms": b["p99_ms"], "batched_GB/s": b["GB/s"],
+                      "per_call_best_GB/s_at_equal_or_lower_p99": best["GB/s"] if best else None,
+                      "per_call_p99_ms": best["p99_ms"] if best else None,
+                      "throughput_ratio": round(b["GB/s"] / best["GB/s"], 2) if best else None})
+    iso = {"per_call_sweep": sweep, "curve": curve}
     print(json.dumps({"workload": "serving: Poisson arrivals of config-3 requests + 5% n=256 k=192 1MiB-shard tail, "
                                   "32 GiB admission cap",
                       "capacity_GB/s": {"batched": cap_b["GB/s"], "per_call": cap_p["GB/s"]},
