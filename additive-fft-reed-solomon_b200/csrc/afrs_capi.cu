@@ -84,20 +84,26 @@ int check_positions(uint32_t n, const uint8_t* pos, size_t e) {
   return AFRS_OK;
 }
 
-// Makes `dev` current for the call.  cudaSetDevice runs even when `dev` is
-// already the thread's device: in a host thread that has made no CUDA call
-// yet it binds the device's context, without which cudaPointerGetAttributes
-// reports page-locked memory without its device address.
+// Makes `dev` current for the call.  cudaSetDevice runs at least once per
+// host thread and device even when `dev` is already the thread's device: in
+// a thread that has made no CUDA call yet it binds the device's context,
+// without which cudaPointerGetAttributes reports page-locked memory without
+// its device address.  After that it runs only when the device changes
+// (it costs a fraction of a microsecond on every small call otherwise).
 struct DeviceGuard {
   int prev = -1;
+  bool moved = false;
   explicit DeviceGuard(int dev) {
+    thread_local int bound = -1;
     cudaGetDevice(&prev);
-    cudaSetDevice(dev);
+    if (prev != dev || bound != dev) {
+      cudaSetDevice(dev);
+      bound = dev;
+      moved = prev != dev;
+    }
   }
   ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    if (moved && prev >= 0) cudaSetDevice(prev);
   }
 };
 
@@ -177,6 +183,7 @@ int encode_route(const afrs_ctx* c, const afrs::EncodeArgs& a) {
   const bool compact = !a.pitch || a.pitch == a.L;
   int r = c->route >= 0 ? c->route : afrs::route_encode(a.n, a.t, a.L);
   if (r < 0) return compact && generic_encode_wins(a) ? afrs::kRouteGeneric : -1;
+  if (r == afrs::kRouteFused && !afrs::fused_encode_shape(a.n, a.t)) return afrs::kRouteSpecial;
   return r == afrs::kRouteGeneric && !compact ? afrs::kRouteSpecial : r;
 }
 
@@ -187,10 +194,11 @@ int launch_encode(afrs_ctx* c, const afrs::EncodeArgs& a0, cudaStream_t s) {
     return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "encode launch");
   }
   afrs::EncodeArgs a = a0;
-  if (route >= 0) a.layout = route == afrs::kRouteSpecialSplit ? 1 : 0;  // else the launcher's rule
+  if (route >= 0)  // else the launcher's rule
+    a.layout = route == afrs::kRouteSpecialSplit ? 1 : (route == afrs::kRouteFused ? afrs::kLayoutFused : 0);
   afrs::ScratchArena sc{nullptr, 0};
   cudaError_t e = cudaSuccess;
-  const size_t need = afrs::scratch_bytes_encode(a.n, a.t, a.L);
+  const size_t need = route == afrs::kRouteFused ? 0 : afrs::scratch_bytes_encode(a.n, a.t, a.L);
   if (need && (e = acquire_work(c, need, s, &sc)) != cudaSuccess) return cuda_fail(e, "encode scratch");
   e = afrs::launch_encode_special(a, sc, s);
   if (e == cudaErrorNotSupported) e = afrs::launch_encode_generic(a, s);
@@ -209,17 +217,21 @@ int recover_route(const afrs_ctx* c, const afrs::RecoverArgs& a) {
   const bool compact = !a.pitch || a.pitch == a.L;
   int r = c->route >= 0 ? c->route : afrs::route_recover(a.n, a.L);
   if (r < 0) r = generic_recover_wins(a) ? afrs::kRouteGeneric : afrs::kRouteSpecial;
+  if (r == afrs::kRouteFused && !afrs::fused_recover_shape(a.n)) return afrs::kRouteSpecial;
   return r == afrs::kRouteGeneric && !compact ? afrs::kRouteSpecial : r;
 }
 
-int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a, cudaStream_t s) {
-  if (recover_route(c, a) == afrs::kRouteGeneric) {
-    cudaError_t e = afrs::launch_recover_generic(a, s);
+int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a0, cudaStream_t s) {
+  const int route = recover_route(c, a0);
+  if (route == afrs::kRouteGeneric) {
+    cudaError_t e = afrs::launch_recover_generic(a0, s);
     return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "recover launch");
   }
+  afrs::RecoverArgs a = a0;
+  if (route == afrs::kRouteFused) a.layout = afrs::kLayoutFused;
   afrs::ScratchArena sc{nullptr, 0};
   cudaError_t e = cudaSuccess;
-  const size_t need = afrs::scratch_bytes_recover(a.n, a.L);
+  const size_t need = route == afrs::kRouteFused ? 0 : afrs::scratch_bytes_recover(a.n, a.L);
   if (need && (e = acquire_work(c, need, s, &sc)) != cudaSuccess) return cuda_fail(e, "recover scratch");
   e = afrs::launch_recover_special(a, sc, s);
   if (e == cudaErrorNotSupported) e = afrs::launch_recover_generic(a, s);
@@ -463,7 +475,7 @@ int afrs_ctx_set_work_cap(afrs_ctx* c, size_t bytes) {
 
 int afrs_ctx_set_route(afrs_ctx* c, int route) {
   if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
-  if (route < AFRS_ROUTE_TABLE || route > AFRS_ROUTE_SPECIAL_SPLIT)
+  if (route < AFRS_ROUTE_TABLE || route > AFRS_ROUTE_FUSED)
     return fail(AFRS_EINVAL, "route %d is not an AFRS_ROUTE_* value", route);
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   c->route = route == AFRS_ROUTE_TABLE ? -1 : route - AFRS_ROUTE_GENERIC;

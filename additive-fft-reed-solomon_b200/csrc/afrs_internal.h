@@ -15,6 +15,9 @@ struct RecoverArgs {
   int n, t, e;       // shards, parity shards, erasures
   uint8_t pos[256];  // erased positions (first e entries)
   size_t pitch = 0;  // bytes between rows; 0 = L (the special kernels honour it)
+  // n = 32 .. 128: kLayoutFused = one launch per call (the whole decoder per
+  // CTA), else the three phase kernels.
+  int layout = -1;
 };
 
 struct EncodeArgs {
@@ -26,8 +29,11 @@ struct EncodeArgs {
   size_t pitch = 0;  // bytes between rows of msg and parity; 0 = L
   // t <= 16 encodes with several chunks: 1 = the warps of a CTA split one
   // slice's chunks, 0 = one warp per slice, -1 = chosen by the built-in rule.
+  // t = 32, 64: kLayoutFused = one launch per call, else the phase kernels.
   int layout = -1;
 };
+// Layout value of the one-launch form of the specialised kernels.
+constexpr int kLayoutFused = 2;
 template <class A>
 __host__ __device__ inline size_t row_pitch(const A& a) {
   return a.pitch ? a.pitch : a.L;
@@ -72,7 +78,10 @@ cudaError_t launch_count_nonzero(const uint8_t* src, size_t len, unsigned long l
 // Per-call kernel routes (route.cu): the tuned table (route_table.inc,
 // written by tune.py) for a shape and shard-length bucket, or -1 when it has
 // no entry (the built-in rules decide).
-enum Route : int { kRouteGeneric = 0, kRouteSpecial = 1, kRouteSpecialSplit = 2 };
+enum Route : int { kRouteGeneric = 0, kRouteSpecial = 1, kRouteSpecialSplit = 2, kRouteFused = 3 };
+// Shapes the one-launch specialised form (kRouteFused) covers.
+inline bool fused_encode_shape(int n, int t) { return (t == 32 || t == 64) && t < n; }
+inline bool fused_recover_shape(int n) { return n >= 32 && n <= 128; }
 int route_encode(int n, int t, size_t L);
 int route_recover(int n, size_t L);
 // Bucket of a shard length in the table: 0 for L <= 64, else ceil(log2 L) - 6;
@@ -101,6 +110,10 @@ void set_last_error(const char* msg);
 // Adds k to the process-wide count of kernels this library has launched
 // (read back with afrs_kernel_launches()).
 void count_launches(unsigned k);
+// Raises kernel fn's dynamic shared-memory limit on the current device to at
+// least `bytes`; the runtime call is made once per kernel, device and larger
+// size (it costs about a microsecond, which small per-call launches notice).
+cudaError_t ensure_smem_attr(const void* fn, size_t bytes);
 size_t scratch_bytes_recover(int n, size_t L);
 
 // Grouped launches of many codewords of one shape (afrs_batch_dev): op 0 =

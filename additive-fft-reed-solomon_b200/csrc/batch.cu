@@ -83,7 +83,7 @@ cudaError_t launch_batch(const BatchLaunch& b, cudaStream_t s) {
   }
   if (b.ntasks == 0) return cudaSuccess;
   const size_t smem = batch_smem_bytes(b.max_rows);
-  e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  e = ensure_smem_attr(reinterpret_cast<const void*>(k_batch), smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);

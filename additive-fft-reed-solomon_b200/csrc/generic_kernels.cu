@@ -4,6 +4,10 @@
 // parallel sweeps over that tile.  These kernels are the coverage path; the
 // shapes that matter for throughput have compile-time-twiddle kernels in
 // special_kernels.cu.
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "afrs_internal.h"
 #include "generic_tile.cuh"
 
@@ -85,9 +89,7 @@ __global__ void k_scale(const uint8_t* src, uint8_t* dst, size_t len, uint8_t c)
 
 size_t slices(size_t L) { return (L + 32 * kCW - 1) / (32 * kCW); }
 
-cudaError_t set_smem(const void* fn, size_t bytes) {
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
+cudaError_t set_smem(const void* fn, size_t bytes) { return ensure_smem_attr(fn, bytes); }
 
 // dst ^= src over len bytes.
 __global__ void k_xor_into(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, size_t len) {
@@ -184,6 +186,20 @@ cudaError_t launch_scale(const uint8_t* src, uint8_t* dst, size_t len, uint8_t c
   k_scale<<<(unsigned)blocks, 256, 0, s>>>(src, dst, len, c);
   count_launches(1);
   return cudaGetLastError();
+}
+
+cudaError_t ensure_smem_attr(const void* fn, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> set;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& have = set[{fn, dev}];
+  if (bytes <= have) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
 }
 
 }  // namespace afrs

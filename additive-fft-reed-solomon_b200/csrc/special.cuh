@@ -459,22 +459,26 @@ struct Split {
   static constexpr size_t kStage = (size_t)RW * 32 * kSplitThreads;
 };
 
+// Stage slot of row i (half hf) of thread tid in a CTA of NT threads.
+template <int NT = kSplitThreads>
 __device__ __forceinline__ uint4* sl(uint32_t* st, int i, int hf, int tid) {
-  return reinterpret_cast<uint4*>(st) + (i * 2 + hf) * kSplitThreads + tid;
+  return reinterpret_cast<uint4*>(st) + (i * 2 + hf) * NT + tid;
 }
+template <int NT = kSplitThreads>
 __device__ __forceinline__ void s_get(uint32_t* st, int i, int tid, uint32_t (&x)[8]) {
-  const uint4 a = *sl(st, i, 0, tid), b = *sl(st, i, 1, tid);
+  const uint4 a = *sl<NT>(st, i, 0, tid), b = *sl<NT>(st, i, 1, tid);
   x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
   x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
 }
+template <int NT = kSplitThreads>
 __device__ __forceinline__ void s_put(uint32_t* st, int i, int tid, const uint32_t (&x)[8]) {
-  *sl(st, i, 0, tid) = make_uint4(x[0], x[1], x[2], x[3]);
-  *sl(st, i, 1, tid) = make_uint4(x[4], x[5], x[6], x[7]);
+  *sl<NT>(st, i, 0, tid) = make_uint4(x[0], x[1], x[2], x[3]);
+  *sl<NT>(st, i, 1, tid) = make_uint4(x[4], x[5], x[6], x[7]);
 }
 
 // Rows first_row + i (i < RW) of colword w into the calling thread's slots
 // (cp.async where 16-byte aligned and in bounds); bit i of skip stages zero.
-template <int RW>
+template <int RW, int NT = kSplitThreads>
 __device__ __forceinline__ void stage_rows(uint32_t* st, const uint8_t* base, size_t first_row, size_t pitch,
                                            size_t L, size_t w, uint32_t skip) {
   const size_t c = cw_col(w);
@@ -483,7 +487,7 @@ __device__ __forceinline__ void stage_rows(uint32_t* st, const uint8_t* base, si
   for (int i = 0; i < RW; i++) {
 #pragma unroll
     for (int hf = 0; hf < 2; hf++) {
-      uint4* dst = sl(st, i, hf, tid);
+      uint4* dst = sl<NT>(st, i, hf, tid);
       if ((skip >> i) & 1) {
         *dst = make_uint4(0, 0, 0, 0);
         continue;
@@ -504,22 +508,22 @@ __device__ __forceinline__ void stage_rows(uint32_t* st, const uint8_t* base, si
 
 // CTA-uniform: every thread publishes its rows in its own slots.  The leading
 // barrier orders it after all earlier reads of the stage.
-template <int RW>
+template <int RW, int NT = kSplitThreads>
 __device__ __forceinline__ void xchg_put(uint32_t* st, const uint32_t (&x)[RW][8]) {
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < RW; i++) s_put(st, i, threadIdx.x, x[i]);
+  for (int i = 0; i < RW; i++) s_put<NT>(st, i, threadIdx.x, x[i]);
   __syncthreads();
 }
 
 // Cross-warp IFFT level: (g0, g1) = (row i of the low warp, row i of the high
 // warp) -> (g0 + T (g0 + g1), g0 + g1); H = 1 for the high warp.
-template <int TW, int H, int RW>
+template <int TW, int H, int RW, int NT = kSplitThreads>
 __device__ __forceinline__ void combine_ifft(uint32_t* st, uint32_t (&x)[RW][8], int ptid) {
 #pragma unroll
   for (int i = 0; i < RW; i++) {
     uint32_t y[8];
-    s_get(st, i, ptid, y);
+    s_get<NT>(st, i, ptid, y);
     if constexpr (H == 0) {
       uint32_t d[8];
 #pragma unroll
@@ -533,12 +537,12 @@ __device__ __forceinline__ void combine_ifft(uint32_t* st, uint32_t (&x)[RW][8],
 }
 
 // Cross-warp FFT level: (a, b) -> (a + T b, a + (T + 1) b).
-template <int TW, int H, int RW>
+template <int TW, int H, int RW, int NT = kSplitThreads>
 __device__ __forceinline__ void combine_fft(uint32_t* st, uint32_t (&x)[RW][8], int ptid) {
 #pragma unroll
   for (int i = 0; i < RW; i++) {
     uint32_t y[8];
-    s_get(st, i, ptid, y);
+    s_get<NT>(st, i, ptid, y);
     if constexpr (H == 0) {
       if constexpr (TW != 0) mul_xor_c<static_cast<uint8_t>(TW)>(x[i], y);
     } else {
@@ -1034,6 +1038,194 @@ __global__ void __launch_bounds__(kSplitThreads, 4)
   rec_b3_body<LOGN>(a, bt, blockIdx.x, gl.g[blockIdx.y], st, loc);
 }
 
+// ---- one launch per call for short shards ---------------------------------
+// Encodes with t = 32 or 64 and recovers with n = 32 .. 128: one CTA per
+// 1024-column slice holds every row of a transform for its 32 colwords, 8
+// rows per warp (t / 8 or n / 8 warps).  Levels 0..2 run inside a warp and
+// the higher ones pair warps through shared memory, as level 3 does in the
+// bottom passes; there is no scratch and no second launch.  Every warp runs
+// its own compile-time variant of each level, so a CTA fetches the code of
+// all of them: the route table picks this form where the three dependent
+// launches and scratch round trips of the phase kernels cost more (short
+// shards).  A partial last slice is handled by the bounds of the row loads
+// and stores.
+template <int ROWS>
+constexpr int fused_threads() {
+  return ROWS / kRowsPerWarp * 32;
+}
+template <int ROWS>
+constexpr size_t fused_smem() {
+  return (size_t)kRowsPerWarp * 32 * fused_threads<ROWS>();
+}
+
+// IFFT levels [3, LOG) at coset BETA over the warps of the CTA (warp q holds
+// rows 8q .. 8q + 7 of the transform).
+template <int LOG, int BETA, int NT>
+__device__ __forceinline__ void fused_ifft_top(uint32_t* st, uint32_t (&x)[kRowsPerWarp][8], int q) {
+  constexpr int RW = kRowsPerWarp, NW = NT / 32;
+  static_for<LOG - 3>([&](auto jj) {
+    constexpr int J = 3 + decltype(jj)::value;
+    xchg_put<RW, NT>(st, x);
+    dispatch<0, NW - 1>(q, [&](auto vv) {
+      constexpr int Q = decltype(vv)::value;
+      constexpr int TW = twiddle_c(J, static_cast<uint8_t>(BETA), (RW * Q) & ~((2 << J) - 1));
+      combine_ifft<TW, (Q >> (J - 3)) & 1, RW, NT>(st, x, threadIdx.x ^ (32 << (J - 3)));
+    });
+  });
+}
+
+// FFT levels LOG - 1 .. 3 at coset 0 over the warps of the CTA.
+template <int LOG, int NT>
+__device__ __forceinline__ void fused_fft_top(uint32_t* st, uint32_t (&x)[kRowsPerWarp][8], int q) {
+  constexpr int RW = kRowsPerWarp, NW = NT / 32;
+  static_for<LOG - 3>([&](auto jj) {
+    constexpr int J = LOG - 1 - decltype(jj)::value;
+    xchg_put<RW, NT>(st, x);
+    dispatch<0, NW - 1>(q, [&](auto vv) {
+      constexpr int Q = decltype(vv)::value;
+      constexpr int TW = twiddle_c(J, 0, (RW * Q) & ~((2 << J) - 1));
+      combine_fft<TW, (Q >> (J - 3)) & 1, RW, NT>(st, x, threadIdx.x ^ (32 << (J - 3)));
+    });
+  });
+}
+
+// Rows row0 .. row0 + 7 of `base` (colword w) into x, bit-sliced; the rows
+// with a bit set in `skip` are zero.  Starts with a barrier (the stage may
+// still be read by partner warps).
+template <int NT>
+__device__ __forceinline__ void fused_load(uint32_t* st, const uint8_t* base, size_t row0, size_t pitch, size_t L,
+                                           size_t w, uint32_t skip, uint32_t (&x)[kRowsPerWarp][8],
+                                           const ShiftMul& km) {
+  constexpr int RW = kRowsPerWarp;
+  __syncthreads();
+  stage_rows<RW, NT>(st, base, row0, pitch, L, w, skip);
+#pragma unroll 1
+  for (int i = 0; i < RW; i++) {
+    uint32_t y[8];
+    s_get<NT>(st, i, threadIdx.x, y);
+    transpose8f(y, km);
+    s_put<NT>(st, i, threadIdx.x, y);
+  }
+#pragma unroll
+  for (int i = 0; i < RW; i++) s_get<NT>(st, i, threadIdx.x, x[i]);
+}
+
+// codec.rs:241-265 in one launch: parity = FFT_t(parity_in? + sum_c
+// IFFT_t(chunk c, omega_ct), 0), the accumulator in registers.
+template <int LOGN, int LOGT>
+__device__ __forceinline__ void enc_fused_body(const EncodeArgs& a, unsigned bx, uint32_t* st) {
+  constexpr int RW = kRowsPerWarp, T = 1 << LOGT, C = (1 << LOGN) / T - 1;
+  constexpr int NT = fused_threads<T>(), NW = NT / 32;
+  const int tid = threadIdx.x, q = tid >> 5;
+  const size_t w = (size_t)bx * 32 + (tid & 31);
+  const ShiftMul km = make_shift_mul();
+  uint32_t acc[RW][8];
+  static_for<C>([&](auto cc) {
+    constexpr int c = decltype(cc)::value + 1;
+    uint32_t x[RW][8];
+    fused_load<NT>(st, a.msg, (size_t)(c - 1) * T + RW * q, row_pitch(a), a.L, w, 0, x, km);
+    dispatch<0, NW - 1>(q, [&](auto vv) { block_ifft<0, 3, decltype(vv)::value, omega_c(c * T), RW>(x); });
+    fused_ifft_top<LOGT, omega_c(c * T), NT>(st, x, q);
+#pragma unroll
+    for (int i = 0; i < RW; i++)
+#pragma unroll
+      for (int p = 0; p < 8; p++) acc[i][p] = c == 1 ? x[i][p] : acc[i][p] ^ x[i][p];
+  });
+  if (a.accumulate) {
+    uint32_t x[RW][8];
+    fused_load<NT>(st, a.parity, (size_t)RW * q, row_pitch(a), a.L, w, 0, x, km);
+#pragma unroll
+    for (int i = 0; i < RW; i++)
+#pragma unroll
+      for (int p = 0; p < 8; p++) acc[i][p] ^= x[i][p];
+  }
+  fused_fft_top<LOGT, NT>(st, acc, q);
+  dispatch<0, NW - 1>(q, [&](auto vv) { block_fft<0, 3, decltype(vv)::value, 0, RW>(acc); });
+  __syncthreads();  // partners' reads of the stage are done
+#pragma unroll
+  for (int i = 0; i < RW; i++) s_put<NT>(st, i, tid, acc[i]);
+#pragma unroll 1
+  for (int i = 0; i < RW; i++) {
+    uint32_t y[8];
+    s_get<NT>(st, i, tid, y);
+    gstore(a.parity, (size_t)RW * q + i, row_pitch(a), a.L, w, y, km);
+  }
+}
+
+// The decoder of the three recover phases in one launch: y = lambda .* r,
+// c = IFFT_n(y), (I + D) c, FFT_n, Forney on the erased rows (whose y is
+// zero, so the identity term adds nothing there).
+template <int LOGN>
+__device__ __forceinline__ void rec_fused_body(const RecoverArgs& a, unsigned bx, uint32_t* st, const LocTable& loc) {
+  constexpr int RW = kRowsPerWarp, NT = fused_threads<(1 << LOGN)>(), NW = NT / 32;
+  const int tid = threadIdx.x, q = tid >> 5, row0 = RW * q;
+  const size_t w = (size_t)bx * 32 + (tid & 31);
+  const ShiftMul km = make_shift_mul();
+  uint32_t x[RW][8];
+  uint32_t skip = 0;
+#pragma unroll
+  for (int i = 0; i < RW; i++) skip |= (uint32_t)(loc.er[row0 + i] != 0) << i;
+  stage_rows<RW, NT>(st, a.rx, row0, row_pitch(a), a.L, w, skip);
+#pragma unroll 1
+  for (int i = 0; i < RW; i++) {
+    if ((skip >> i) & 1) continue;
+    uint32_t y[8];
+    s_get<NT>(st, i, tid, y);
+    transpose8f(y, km);
+    scale_log(y, loc.lam[row0 + i]);
+    s_put<NT>(st, i, tid, y);
+  }
+#pragma unroll
+  for (int i = 0; i < RW; i++) s_get<NT>(st, i, tid, x[i]);
+  dispatch<0, NW - 1>(q, [&](auto vv) { block_ifft<0, 3, decltype(vv)::value, 0, RW>(x); });
+  fused_ifft_top<LOGN, 0, NT>(st, x, q);
+  // (I + D): the in-warp bits in registers; for each warp bit clear in this
+  // warp's rows, the original rows of the partner warp that has it set.
+  __syncthreads();  // partners' reads of the stage are done
+#pragma unroll
+  for (int i = 0; i < RW; i++) s_put<NT>(st, i, tid, x[i]);
+  __syncthreads();
+  one_plus_derivative<RW>(x);
+#pragma unroll
+  for (int j = 3; j < LOGN; j++) {
+    if ((q >> (j - 3)) & 1) continue;
+    const int ptid = tid ^ (32 << (j - 3));
+#pragma unroll
+    for (int i = 0; i < RW; i++) {
+      uint32_t y[8];
+      s_get<NT>(st, i, ptid, y);
+#pragma unroll
+      for (int p = 0; p < 8; p++) x[i][p] ^= y[p];
+    }
+  }
+  fused_fft_top<LOGN, NT>(st, x, q);
+  dispatch<0, NW - 1>(q, [&](auto vv) { block_fft<0, 3, decltype(vv)::value, 0, RW>(x); });
+  __syncthreads();  // partners' reads of the stage are done
+#pragma unroll
+  for (int i = 0; i < RW; i++) s_put<NT>(st, i, tid, x[i]);
+#pragma unroll 1
+  for (int i = 0; i < RW; i++) {
+    const int r = row0 + i;
+    if (!loc.er[r]) continue;
+    uint32_t y[8];
+    s_get<NT>(st, i, tid, y);
+    scale_log(y, loc.ilp[r]);
+    gstore(a.rx, (size_t)r, row_pitch(a), a.L, w, y, km);
+  }
+}
+
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(fused_threads<(1 << LOGT)>(), 1) k_enc_fused(EncodeArgs a) {
+  extern __shared__ uint32_t st[];
+  enc_fused_body<LOGN, LOGT>(a, blockIdx.x, st);
+}
+template <int LOGN>
+__global__ void __launch_bounds__(fused_threads<(1 << LOGN)>(), 1)
+    k_rec_fused(RecoverArgs a, const __grid_constant__ LocTable loc) {
+  extern __shared__ uint32_t st[];
+  rec_fused_body<LOGN>(a, blockIdx.x, st, loc);
+}
+
 // Grouped recover (see EncJob): gmask bit g is set when row group g holds an
 // erasure of this codeword; the last pass runs only those groups.
 struct RecJob {
@@ -1132,7 +1324,7 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
     const size_t smem = enc_small_smem<LOGN, LOGT>(split);
     auto fn = split ? k_enc_small<LOGN, LOGT, true> : k_enc_small<LOGN, LOGT, false>;
     if (smem > (48 << 10)) {
-      cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(fn), smem);
       if (e != cudaSuccess) return e;
     }
     fn<<<enc_small_ctas<LOGN, LOGT>(slices, split), kThreads, smem, s>>>(a);
@@ -1140,6 +1332,19 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
     return cudaGetLastError();
   } else {
     constexpr int N = 1 << LOGN, T = 1 << LOGT, C = N / T - 1, G = T / 16;
+    if constexpr (LOGT == 5 || LOGT == 6) {
+      const size_t slices = (a.L + 1023) / 1024;
+      if (a.layout == kLayoutFused && slices <= 0x7fffffff) {
+        constexpr size_t smem = fused_smem<T>();
+        if constexpr (smem > (48 << 10)) {
+          cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(k_enc_fused<LOGN, LOGT>), smem);
+          if (e != cudaSuccess) return e;
+        }
+        k_enc_fused<LOGN, LOGT><<<(unsigned)slices, fused_threads<T>(), smem, s>>>(a);
+        count_launches(1);
+        return cudaGetLastError();
+      }
+    }
     const size_t total_cw = total_colwords(a.L);
     const size_t bcw = batch_colwords(N - T, 1, sc.bytes, total_cw);
     if (bcw == 0) return cudaErrorMemoryAllocation;
@@ -1169,6 +1374,19 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
     return cudaGetLastError();
   } else {
     constexpr int N = 1 << LOGN, G = N / 16;
+    if constexpr (LOGN <= 7) {
+      const size_t slices = (a.L + 1023) / 1024;
+      if (a.layout == kLayoutFused && slices <= 0x7fffffff) {
+        constexpr size_t smem = fused_smem<N>();
+        if constexpr (smem > (48 << 10)) {
+          cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(k_rec_fused<LOGN>), smem);
+          if (e != cudaSuccess) return e;
+        }
+        k_rec_fused<LOGN><<<(unsigned)slices, fused_threads<N>(), smem, s>>>(a, cached_locator(a));
+        count_launches(1);
+        return cudaGetLastError();
+      }
+    }
     GroupList gl{};
     bool has[16] = {};
     for (int j = 0; j < a.e; j++) has[a.pos[j] >> 4] = true;
@@ -1207,7 +1425,7 @@ cudaError_t launch_enc_jobs(const EncJob* d, int count, size_t max_ncw, cudaStre
     const size_t smem = enc_small_smem<LOGN, LOGT>(split);
     auto fn = split ? k_enc_small_jobs<LOGN, LOGT, true> : k_enc_small_jobs<LOGN, LOGT, false>;
     if (smem > (48 << 10)) {
-      cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(fn), smem);
       if (e != cudaSuccess) return e;
     }
     for (int j0 = 0; j0 < count; j0 += 65535) {

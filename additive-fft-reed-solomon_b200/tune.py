@@ -6,8 +6,9 @@ For every encode shape (n, t), recover shape n and shard-length bucket
 (L = 64 B, 128 B, ..., 4 MiB: bucket b covers 64 * 2^(b-1) < L <= 64 * 2^b)
 it times, at the bucket's largest length, each route the C ABI can force
 (afrs_ctx_set_route): the one-launch generic kernel, the specialised
-kernels, and for t <= 16 encodes with more than one chunk both layouts of the
-specialised kernel.  A call is timed as CUDA-graph replays of 10 calls on
+kernels, for t <= 16 encodes with more than one chunk both layouts of the
+specialised kernel, and for the shapes it covers (encodes with t = 32, 64;
+recovers with n = 32 .. 128) the specialised kernels fused into one launch.  A call is timed as CUDA-graph replays of 10 calls on
 device buffers (no host overhead), best of 3.  The fastest route wins; the
 built-in rule's route is kept when it is within 3 % of the fastest.
 Codewords above --max-bytes are not measured (the table entry stays -1 and
@@ -118,7 +119,7 @@ def main():
             pos = list(range(0, n, 2))
             codec = afrs.Codec(n, t, context=ctx)
             times = {}
-            for route in (0, 1):
+            for route in (0, 1, 3) if 32 <= n <= 128 else (0, 1):
                 ctx.set_route(route + lib.AFRS_ROUTE_GENERIC)
                 times[route] = timed(lambda: codec.recover_erasure_shards(rx, None, L, pos))
             rec[ln][b] = choose(times, builtin_recover_route(n, L))
@@ -128,6 +129,8 @@ def main():
                 msg, par = big[:(n - t) * L], big2[:t * L]
                 codec = afrs.Codec(n, t, context=ctx)
                 routes = (0, 1, 2) if t <= 16 and n // t - 1 > 1 else (0, 1)
+                if t in (32, 64):
+                    routes += (3,)
                 times = {}
                 for route in routes:
                     ctx.set_route(route + lib.AFRS_ROUTE_GENERIC)
@@ -145,12 +148,14 @@ def main():
         "// -1 = not measured.  Regenerate with",
         "//   python additive-fft-reed-solomon_b200/tune.py",
         f"constexpr int kRouteBuckets = {BUCKETS};  // L <= 64, <= 128, ..., <= 4 MiB",
-        "// [log2 n][log2 t][bucket]: 0 generic, 1 specialised, 2 specialised with split chunks",
+        "// [log2 n][log2 t][bucket]: 0 generic, 1 specialised, 2 specialised with split chunks,",
+        "// 3 specialised in one launch",
         f"const int8_t kEncRoute[9][9][{BUCKETS}] = {{",
     ]
     for ln in range(9):
         lines.append("    {" + ", ".join("{" + ", ".join(str(v) for v in enc[ln][lt]) + "}" for lt in range(9)) + "},")
-    lines += ["};", "// [log2 n][bucket]: 0 generic, 1 specialised", f"const int8_t kRecRoute[9][{BUCKETS}] = {{"]
+    lines += ["};", "// [log2 n][bucket]: 0 generic, 1 specialised, 3 specialised in one launch",
+              f"const int8_t kRecRoute[9][{BUCKETS}] = {{"]
     for ln in range(9):
         lines.append("    {" + ", ".join(str(v) for v in rec[ln]) + "},")
     lines.append("};")

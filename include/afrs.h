@@ -207,13 +207,16 @@ int afrs_ctx_set_work_cap(afrs_ctx* ctx, size_t bytes);
  * kernels with compile-time twiddles, t <= 16 encodes with one warp per
  * 1024-column slice; SPECIAL_SPLIT, the same with the warps of a CTA
  * splitting one slice's chunks (t <= 16 encodes with n > 2t; otherwise as
- * SPECIAL).  Results are identical on every route.  No counterpart in the
- * reference, whose kernel choice is a build-time CPU feature test
- * (rs/build.rs:628-646). */
+ * SPECIAL); FUSED, the compile-time-twiddle kernels in one launch per call,
+ * one CTA holding every row of a 1024-column slice (encodes with t = 32 or
+ * 64, recovers with n = 32 .. 128; otherwise as SPECIAL).  Results are
+ * identical on every route.  No counterpart in the reference, whose kernel
+ * choice is a build-time CPU feature test (rs/build.rs:628-646). */
 #define AFRS_ROUTE_TABLE 0
 #define AFRS_ROUTE_GENERIC 1
 #define AFRS_ROUTE_SPECIAL 2
 #define AFRS_ROUTE_SPECIAL_SPLIT 3
+#define AFRS_ROUTE_FUSED 4
 int afrs_ctx_set_route(afrs_ctx* ctx, int route);
 
 /* Number of CUDA kernels this library has launched in this process, over
