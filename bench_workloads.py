@@ -374,6 +374,10 @@ def run_kernels(args):
     recover_case("recover_generic", 16, 8, 1 << 20, lib.AFRS_ROUTE_GENERIC, "k_recover_generic")
     recover_case("rec_small", 16, 8, 1 << 20, lib.AFRS_ROUTE_SPECIAL, "k_rec_small<4>")
     recover_case("recover_phases_n64", 64, 32, 262144, lib.AFRS_ROUTE_SPECIAL, "k_rec_b1/p2/b3<6>")
+    encode_case("encode_fused_t32", 64, 32, 262144, lib.AFRS_ROUTE_FUSED, "k_enc_fused<6,5>")
+    recover_case("recover_fused_n32", 32, 16, 524288, lib.AFRS_ROUTE_FUSED, "k_rec_fused<5>")
+    recover_case("recover_fused_n64", 64, 32, 262144, lib.AFRS_ROUTE_FUSED, "k_rec_fused<6>")
+    recover_case("recover_phases_n32", 32, 16, 524288, lib.AFRS_ROUTE_SPECIAL, "k_rec_b1/p2/b3<5>")
 
     # Batched path: 256 small mixed jobs share the generic persistent kernel
     # (every shape group is below the grouping threshold); two large shape
