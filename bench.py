@@ -132,6 +132,23 @@ def cpu_per_pair() -> float:
     return _PER_PAIR
 
 
+def host_cpu() -> dict:
+    """Model and vector features of the host cores the CPU baseline runs on."""
+    model, flags = "unknown", set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                key, _, val = line.partition(":")
+                key = key.strip()
+                if key == "model name" and model == "unknown":
+                    model = val.strip()
+                elif key == "flags" and not flags:
+                    flags = set(val.split())
+    except OSError:
+        pass
+    return {"cpu": model, "gfni": "gfni" in flags, "avx512f": "avx512f" in flags}
+
+
 def cpu_baseline(seconds: float, threads: int):
     """GFNI restatement of the reference's kernel + codec on host cores, on a
     bounded sample of the same workload (same n, t, L): about `seconds` of
@@ -197,7 +214,8 @@ def run_reference(args):
                    "shard_len": SHARD_LEN, "erasures": T_PARITY},
         "encode_gbs": round(enc, 3), "recover_gbs": round(rec, 3),
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": sample + " (C restatement of rs/src/kernel/gfni_kernel.rs; no Rust toolchain)"},
+                         "sample": sample + " (C restatement of rs/src/kernel/gfni_kernel.rs; no Rust toolchain)",
+                         **host_cpu()},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -534,7 +552,7 @@ def main():
         threads = os.cpu_count() or 1
         v, ce, cr, sample = cpu_baseline(args.cpu_seconds, threads)
         cpu = {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample,
-               "encode_gbs": round(ce, 3), "recover_gbs": round(cr, 3)}
+               "encode_gbs": round(ce, 3), "recover_gbs": round(cr, 3), **host_cpu()}
 
     out = {
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
