@@ -21,7 +21,9 @@
 // straight-line code for n = 256.)
 // Between phases the rows stay bit-sliced in a scratch buffer (1 GiB at most;
 // L2-resident for small codewords); longer shards are processed in column
-// batches.
+// batches.  For some shapes a one-launch form (k_enc_fused, k_rec_fused)
+// holds all rows of a slice in one CTA instead; the route table picks it
+// where it measured faster (short shards).
 // Transforms with k <= 4 run entirely inside one thread.
 #pragma once
 #include <array>
