@@ -288,14 +288,16 @@ def _pinned(a):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n,t,L", [(256, 128, 3 * 16384 + 1000), (64, 16, 2 * 65536 + 77), (16, 8, 300000),
-                                   (256, 32, 16384)])
+                                   (256, 32, 16384), (32, 16, 3 * 131072 + 333), (64, 32, 200000)])
 @pytest.mark.parametrize("pinned", [True, False])
 def test_staged_host_path_windows_and_runs(afrs, n, t, L, pinned):
     """The host-buffer entry points stage column windows (4 MiB per window:
     16 KiB columns at n = 256) through two device slots and copy only the
     rows an operation reads or writes, as merged runs.  Shards spanning
     several windows with a ragged last one, page-locked and pageable buffers,
-    accumulate, and erasure patterns with long runs, isolated rows and gaps."""
+    accumulate, and erasure patterns with long runs, isolated rows and gaps.
+    The windows take the routed kernels: at n = 32 (128 KiB windows) recovers
+    and at n = 64, t = 32 (64 KiB windows) encodes run the one-launch form."""
     msg, par = _codeword(n, t, L, seed=n + L)
     cw = np.concatenate([par, msg])
     codec = afrs.Codec(n, t)
