@@ -811,11 +811,15 @@ constexpr size_t kGroupScratchCap = (size_t)1 << 30;
 // Smallest shape group (sum of n * shard_len) worth its own launches.
 constexpr size_t kGroupMinBytes = (size_t)8 << 20;
 
-// A job of a batch that runs through the grouped phase kernels.
+// A job of a batch that runs through the grouped phase kernels.  The
+// grouped scratch is reused in rounds: the jobs of one round hold at most
+// kGroupScratchCap bytes of it, and a round starts once every group stream
+// has finished the previous one.
 struct GroupedJob {
   size_t job;      // index into the caller's array
   int op, n, t;    // shape key
   size_t scratch;  // byte offset in the batch's grouped scratch
+  int round;       // scratch round
 };
 
 // One batch prepared on the host: which jobs run where, and the layout of
@@ -832,9 +836,11 @@ struct BatchPrep {
   struct Group {
     int op, n, t;
     size_t first, count, desc_off, max_ncw;
+    int round;
   };
   std::vector<Group> groups;
-  size_t grp_bytes = 0;  // grouped scratch
+  int rounds = 0;
+  size_t grp_bytes = 0;  // grouped scratch (the largest round)
   int max_rows = 0;
   size_t o_jobs = 0, o_tasks = 0, o_rec = 0, o_pos = 0, o_cnt = 0, o_loc = 0;
   size_t upload = 0;  // bytes the host writes
@@ -878,26 +884,41 @@ int batch_prepare(afrs_job* jobs, size_t count, BatchPrep* p) {
     p->valid.push_back(i);
   }
   // A shape group (encode: n, t; recover: n) runs on the specialised kernels
-  // when it holds enough bytes to fill the GPU and its scratch fits the
-  // grouped scratch; the rest share one launch of the generic persistent
-  // kernel, which runs concurrently with the groups.
+  // when it holds enough bytes to fill the GPU; its jobs take scratch in
+  // rounds of at most kGroupScratchCap bytes, assigned in shape order so that
+  // a group spans few rounds.  The rest (small groups, shapes without grouped
+  // kernels, a job whose scratch alone exceeds the cap) share one launch of
+  // the generic persistent kernel, which runs concurrently with the groups.
   auto key = [&](const afrs_job& j) {
     return std::make_tuple((int)j.op, (int)j.n, j.op == AFRS_OP_ENCODE ? (int)j.t : 0);
   };
   std::map<std::tuple<int, int, int>, size_t> group_bytes;
   for (size_t i : p->valid) group_bytes[key(jobs[i])] += (size_t)jobs[i].n * jobs[i].shard_len;
+  std::vector<size_t> order(p->valid);
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return key(jobs[x]) < key(jobs[y]); });
+  std::vector<bool> grouped(count, false);
+  size_t round_bytes = 0;
+  for (size_t i : order) {
+    const afrs_job& j = jobs[i];
+    const int op = j.op == AFRS_OP_ENCODE ? 0 : 1;
+    if (!afrs::jobs_supported(op, (int)j.n, (int)j.t) || group_bytes[key(j)] < kGroupMinBytes) continue;
+    const size_t need = align256(afrs::job_scratch_bytes(op, (int)j.n, (int)j.t, j.shard_len));
+    if (need > kGroupScratchCap) continue;
+    if (round_bytes + need > kGroupScratchCap) {
+      p->rounds++;
+      round_bytes = 0;
+    }
+    p->grouped.push_back(GroupedJob{i, op, (int)j.n, std::get<2>(key(j)), round_bytes, p->rounds});
+    round_bytes += need;
+    p->grp_bytes = std::max(p->grp_bytes, round_bytes);
+    grouped[i] = true;
+  }
+  if (!p->grouped.empty()) p->rounds++;
   for (size_t i : p->valid) {
+    if (grouped[i]) continue;
     const afrs_job& j = jobs[i];
     const bool enc = j.op == AFRS_OP_ENCODE;
     const int op = enc ? 0 : 1;
-    if (afrs::jobs_supported(op, (int)j.n, (int)j.t) && group_bytes[key(j)] >= kGroupMinBytes) {
-      const size_t need = align256(afrs::job_scratch_bytes(op, (int)j.n, (int)j.t, j.shard_len));
-      if (p->grp_bytes + need <= kGroupScratchCap) {
-        p->grouped.push_back(GroupedJob{i, op, (int)j.n, std::get<2>(key(j)), p->grp_bytes});
-        p->grp_bytes += need;
-        continue;
-      }
-    }
     afrs::BatchJob b{};
     b.src = j.src;
     b.dst = j.dst;
@@ -923,10 +944,10 @@ int batch_prepare(afrs_job* jobs, size_t count, BatchPrep* p) {
     for (size_t i : p->valid) jobs[i].status = AFRS_EINVAL;
     return fail(AFRS_EINVAL, "too many tiles");
   }
-  // Jobs sorted by shape (stable: caller order within a shape); the
-  // descriptors of one shape group form one array.
+  // Jobs sorted by round and shape (stable: caller order within a shape);
+  // the descriptors of one shape group of a round form one array.
   std::stable_sort(p->grouped.begin(), p->grouped.end(), [](const GroupedJob& x, const GroupedJob& y) {
-    return std::make_tuple(x.op, x.n, x.t) < std::make_tuple(y.op, y.n, y.t);
+    return std::make_tuple(x.round, x.op, x.n, x.t) < std::make_tuple(y.round, y.op, y.n, y.t);
   });
   p->o_jobs = 0;
   p->o_tasks = align256(p->o_jobs + p->bj.size() * sizeof(afrs::BatchJob));
@@ -936,9 +957,10 @@ int batch_prepare(afrs_job* jobs, size_t count, BatchPrep* p) {
   auto& groups = p->groups;
   for (size_t q = 0; q < p->grouped.size(); q++) {
     const GroupedJob& g = p->grouped[q];
-    if (groups.empty() || groups.back().op != g.op || groups.back().n != g.n || groups.back().t != g.t) {
+    if (groups.empty() || groups.back().op != g.op || groups.back().n != g.n || groups.back().t != g.t ||
+        groups.back().round != g.round) {
       if (!groups.empty()) o_grp = align256(o_grp + groups.back().count * afrs::job_desc_bytes(groups.back().op));
-      groups.push_back(BatchPrep::Group{g.op, g.n, g.t, q, 0, o_grp, 0});
+      groups.push_back(BatchPrep::Group{g.op, g.n, g.t, q, 0, o_grp, 0, g.round});
     }
     groups.back().count++;
     groups.back().max_ncw = std::max(groups.back().max_ncw, afrs::job_colwords(jobs[g.job].shard_len));
@@ -1009,10 +1031,21 @@ cudaError_t batch_enqueue(afrs_ctx* c, const BatchPrep& p, uint8_t* d, cudaStrea
     e = afrs::launch_batch(bl, s);
     *what = "batch launch";
   }
-  if (e == cudaSuccess) {
+  // Rounds of grouped jobs: within a round the groups (largest first) go
+  // round-robin to the group streams; a round reuses the previous round's
+  // scratch, so every group stream first waits for all of them.
+  for (int r = 0; r < p.rounds && e == cudaSuccess; r++) {
+    if (r > 0) {
+      *what = "batch round barrier";
+      for (int k = 0; k < nstreams && e == cudaSuccess; k++) e = cudaEventRecord(c->grp_join[k], c->grp_stream[k]);
+      for (int k = 0; k < nstreams && e == cudaSuccess; k++)
+        for (int k2 = 0; k2 < nstreams && e == cudaSuccess; k2++)
+          if (k2 != k) e = cudaStreamWaitEvent(c->grp_stream[k], c->grp_join[k2], 0);
+    }
     const auto& groups = p.groups;
-    std::vector<size_t> order(groups.size());
-    for (size_t q = 0; q < order.size(); q++) order[q] = q;
+    std::vector<size_t> order;
+    for (size_t q = 0; q < groups.size(); q++)
+      if (groups[q].round == r) order.push_back(q);
     std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
       return groups[x].count * groups[x].max_ncw * groups[x].n > groups[y].count * groups[y].max_ncw * groups[y].n;
     });

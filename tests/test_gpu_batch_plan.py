@@ -90,3 +90,62 @@ def test_plan_launch_in_a_cuda_graph(afrs):
             assert (j.dst.cpu().numpy() == r).all()
     del g
     plan.close()
+
+
+@pytest.mark.gpu
+def test_grouped_scratch_rounds(afrs):
+    """A batch whose grouped jobs need more scratch than one round holds
+    (1 GiB): nine n = 256 recovers with 512 KiB shards need 268 MB each, so
+    they run in three rounds that reuse the scratch, next to nine encodes of
+    the same shape.  Each recover must give back its original codeword and
+    each encode the per-call encoder's parity (itself checked against the
+    oracle by the parity tests), through afrs_batch_dev and through a plan
+    launched twice."""
+    n, t, L, K = 256, 128, 512 << 10, 9
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    codec = afrs.Codec(n, t)
+    rng = np.random.default_rng(17)
+    cws, rxs, msgs, pars, patterns = [], [], [], [], []
+    for i in range(K):
+        cw = torch.empty(n * L, dtype=torch.uint8, device="cuda")
+        cw[t * L:] = torch.randint(0, 256, ((n - t) * L,), dtype=torch.uint8, device="cuda", generator=g)
+        codec.encode_parity(cw[t * L:], cw[:t * L], L)
+        pos = sorted(rng.choice(n, t, replace=False).tolist())
+        rx = cw.clone()
+        for p in pos:
+            rx[p * L:(p + 1) * L].zero_()
+        cws.append(cw)
+        rxs.append(rx)
+        patterns.append(pos)
+        msgs.append(cw[t * L:].clone())
+        pars.append(torch.full((t * L,), 0x5A, dtype=torch.uint8, device="cuda"))
+
+    def jobs():
+        out = [afrs.Job.recover(n, t, rxs[i], L, patterns[i]) for i in range(K)]
+        out += [afrs.Job.encode(n, t, msgs[i], pars[i], L) for i in range(K)]
+        return out
+
+    def check():
+        torch.cuda.synchronize()
+        for i in range(K):
+            assert torch.equal(rxs[i], cws[i]), f"recover {i}"
+            assert torch.equal(pars[i], cws[i][:t * L]), f"encode {i}"
+
+    def reset():
+        for i in range(K):
+            for p in patterns[i]:
+                rxs[i][p * L:(p + 1) * L].zero_()
+            pars[i].fill_(0x5A)
+
+    statuses = afrs.run_batch(jobs())
+    assert statuses == [1] * K + [0] * K
+    check()
+    js = jobs()
+    reset()
+    plan = afrs.BatchPlan(js)
+    for _ in range(2):
+        plan.launch()
+        check()
+        reset()
+    plan.close()
