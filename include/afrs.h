@@ -115,7 +115,9 @@ int afrs_scale_dev(afrs_ctx* ctx, const uint8_t* d_src, uint8_t* d_dst, size_t l
  * AFRS_OK once the batch is enqueued on `stream`, or < 0 when nothing was.
  * The descriptor tables and scratch live in the context, in two slots used
  * alternately: batches on different streams may run concurrently, and a call
- * waits on the host until the previous batch of its slot has finished. */
+ * waits on the host until the previous batch of its slot has finished.  A
+ * slot's grouped scratch is at most 1 GiB; a batch that needs more runs its
+ * grouped jobs in rounds that reuse it. */
 #define AFRS_OP_ENCODE 0u
 #define AFRS_OP_RECOVER 1u
 typedef struct afrs_job {
