@@ -28,6 +28,7 @@ AFRS_ROUTE_GENERIC = 1
 AFRS_ROUTE_SPECIAL = 2
 AFRS_ROUTE_SPECIAL_SPLIT = 3
 AFRS_ROUTE_FUSED = 4
+AFRS_ROUTE_FEW = 5
 
 AFRS_OP_ENCODE = 0
 AFRS_OP_RECOVER = 1

@@ -181,7 +181,7 @@ bool generic_encode_wins(const afrs::EncodeArgs& a) {
 // else the built-in rule.  The generic kernel takes compact rows only.
 int encode_route(const afrs_ctx* c, const afrs::EncodeArgs& a) {
   const bool compact = !a.pitch || a.pitch == a.L;
-  int r = c->route >= 0 ? c->route : afrs::route_encode(a.n, a.t, a.L);
+  int r = c->route >= 0 && c->route != afrs::kRouteFew ? c->route : afrs::route_encode(a.n, a.t, a.L);
   if (r < 0) return compact && generic_encode_wins(a) ? afrs::kRouteGeneric : -1;
   if (r == afrs::kRouteFused && !afrs::fused_encode_shape(a.n, a.t)) return afrs::kRouteSpecial;
   return r == afrs::kRouteGeneric && !compact ? afrs::kRouteSpecial : r;
@@ -213,9 +213,16 @@ bool generic_recover_wins(const afrs::RecoverArgs& a) {
   return a.n == 16 && (size_t)a.n * a.L <= ((size_t)4 << 20);
 }
 
+// Recovers of few erasures take the few-erasure kernel where it is faster
+// (few_recover_wins), or wherever it applies when the context forces it: one
+// pass over the survivors with no scratch, where the Leopard form runs two
+// n-point transforms whatever e is.
 int recover_route(const afrs_ctx* c, const afrs::RecoverArgs& a) {
   const bool compact = !a.pitch || a.pitch == a.L;
-  int r = c->route >= 0 ? c->route : afrs::route_recover(a.n, a.L);
+  if (c->route == afrs::kRouteFew ? afrs::few_recover_shape(a.n, a.e)
+                                  : c->route < 0 && afrs::few_recover_wins(a.n, a.e, a.L))
+    return afrs::kRouteFew;
+  int r = c->route >= 0 && c->route != afrs::kRouteFew ? c->route : afrs::route_recover(a.n, a.L);
   if (r < 0) r = generic_recover_wins(a) ? afrs::kRouteGeneric : afrs::kRouteSpecial;
   if (r == afrs::kRouteFused && !afrs::fused_recover_shape(a.n)) return afrs::kRouteSpecial;
   return r == afrs::kRouteGeneric && !compact ? afrs::kRouteSpecial : r;
@@ -228,10 +235,11 @@ int launch_recover(afrs_ctx* c, const afrs::RecoverArgs& a0, cudaStream_t s) {
     return e == cudaSuccess ? AFRS_OK : cuda_fail(e, "recover launch");
   }
   afrs::RecoverArgs a = a0;
-  if (route == afrs::kRouteFused) a.layout = afrs::kLayoutFused;
+  a.layout = route == afrs::kRouteFused ? afrs::kLayoutFused : (route == afrs::kRouteFew ? afrs::kLayoutFew : 0);
   afrs::ScratchArena sc{nullptr, 0};
   cudaError_t e = cudaSuccess;
-  const size_t need = route == afrs::kRouteFused ? 0 : afrs::scratch_bytes_recover(a.n, a.L);
+  const size_t need =
+      route == afrs::kRouteFused || route == afrs::kRouteFew ? 0 : afrs::scratch_bytes_recover(a.n, a.L);
   if (need && (e = acquire_work(c, need, s, &sc)) != cudaSuccess) return cuda_fail(e, "recover scratch");
   e = afrs::launch_recover_special(a, sc, s);
   if (e == cudaErrorNotSupported) e = afrs::launch_recover_generic(a, s);
@@ -475,7 +483,7 @@ int afrs_ctx_set_work_cap(afrs_ctx* c, size_t bytes) {
 
 int afrs_ctx_set_route(afrs_ctx* c, int route) {
   if (!c) return fail(AFRS_EINVAL, "ctx is NULL");
-  if (route < AFRS_ROUTE_TABLE || route > AFRS_ROUTE_FUSED)
+  if (route < AFRS_ROUTE_TABLE || route > AFRS_ROUTE_FEW)
     return fail(AFRS_EINVAL, "route %d is not an AFRS_ROUTE_* value", route);
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   c->route = route == AFRS_ROUTE_TABLE ? -1 : route - AFRS_ROUTE_GENERIC;
@@ -808,8 +816,10 @@ namespace {
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 constexpr size_t kGroupScratchCap = (size_t)1 << 30;
-// Smallest shape group (sum of n * shard_len) worth its own launches.
+// Smallest shape group (sum of n * shard_len) worth its own launches; a
+// few-erasure group needs no scratch and is one launch.
 constexpr size_t kGroupMinBytes = (size_t)8 << 20;
+constexpr size_t kFewGroupMinBytes = (size_t)1 << 20;
 
 // A job of a batch that runs through the grouped phase kernels.  The
 // grouped scratch is reused in rounds: the jobs of one round hold at most
@@ -817,9 +827,10 @@ constexpr size_t kGroupMinBytes = (size_t)8 << 20;
 // has finished the previous one.
 struct GroupedJob {
   size_t job;      // index into the caller's array
-  int op, n, t;    // shape key
+  int op, n, t;    // shape key (op 2, few-erasure recover: t = log2 of its chunk size)
   size_t scratch;  // byte offset in the batch's grouped scratch
   int round;       // scratch round
+  size_t few;      // op 2: offset of its descriptor in BatchPrep::few_desc
 };
 
 // One batch prepared on the host: which jobs run where, and the layout of
@@ -833,6 +844,7 @@ struct BatchPrep {
   std::vector<int> rec;
   std::vector<uint8_t> pos;
   std::vector<GroupedJob> grouped;
+  std::vector<uint8_t> few_desc;  // descriptors of the few-erasure recovers
   struct Group {
     int op, n, t;
     size_t first, count, desc_off, max_ncw;
@@ -889,8 +901,14 @@ int batch_prepare(afrs_job* jobs, size_t count, BatchPrep* p) {
   // a group spans few rounds.  The rest (small groups, shapes without grouped
   // kernels, a job whose scratch alone exceeds the cap) share one launch of
   // the generic persistent kernel, which runs concurrently with the groups.
+  // Recovers of at most 8 erasures with n >= 32 form their own groups (op 2,
+  // keyed by n and the chunk size 2^ceil(log2 e)) on the few-erasure kernel.
   auto key = [&](const afrs_job& j) {
-    return std::make_tuple((int)j.op, (int)j.n, j.op == AFRS_OP_ENCODE ? (int)j.t : 0);
+    if (j.op == AFRS_OP_ENCODE) return std::make_tuple(0, (int)j.n, (int)j.t);
+    if (!afrs::few_recover_shape((int)j.n, (int)j.e)) return std::make_tuple(1, (int)j.n, 0);
+    int lt = 0;
+    while ((1u << lt) < j.e) lt++;
+    return std::make_tuple(2, (int)j.n, lt);
   };
   std::map<std::tuple<int, int, int>, size_t> group_bytes;
   for (size_t i : p->valid) group_bytes[key(jobs[i])] += (size_t)jobs[i].n * jobs[i].shard_len;
@@ -900,15 +918,33 @@ int batch_prepare(afrs_job* jobs, size_t count, BatchPrep* p) {
   size_t round_bytes = 0;
   for (size_t i : order) {
     const afrs_job& j = jobs[i];
-    const int op = j.op == AFRS_OP_ENCODE ? 0 : 1;
-    if (!afrs::jobs_supported(op, (int)j.n, (int)j.t) || group_bytes[key(j)] < kGroupMinBytes) continue;
+    const int op = std::get<0>(key(j));
+    if (!afrs::jobs_supported(op, (int)j.n, (int)j.t) ||
+        group_bytes[key(j)] < (op == 2 ? kFewGroupMinBytes : kGroupMinBytes))
+      continue;
+    size_t few = 0;
+    if (op == 2) {
+      afrs::RecoverArgs a{};
+      a.rx = j.dst;
+      a.L = j.shard_len;
+      a.n = (int)j.n;
+      a.t = (int)j.t;
+      a.e = (int)j.e;
+      std::memcpy(a.pos, j.positions, j.e);
+      few = p->few_desc.size();
+      p->few_desc.resize(few + afrs::job_desc_bytes(2));
+      if (!afrs::fill_few_job(p->few_desc.data() + few, a)) {
+        p->few_desc.resize(few);
+        continue;
+      }
+    }
     const size_t need = align256(afrs::job_scratch_bytes(op, (int)j.n, (int)j.t, j.shard_len));
     if (need > kGroupScratchCap) continue;
     if (round_bytes + need > kGroupScratchCap) {
       p->rounds++;
       round_bytes = 0;
     }
-    p->grouped.push_back(GroupedJob{i, op, (int)j.n, std::get<2>(key(j)), round_bytes, p->rounds});
+    p->grouped.push_back(GroupedJob{i, op, (int)j.n, std::get<2>(key(j)), round_bytes, p->rounds, few});
     round_bytes += need;
     p->grp_bytes = std::max(p->grp_bytes, round_bytes);
     grouped[i] = true;
@@ -987,7 +1023,9 @@ void batch_fill(const BatchPrep& p, const afrs_job* jobs, uint8_t* h, uint8_t* s
       const afrs_job& j = jobs[gj.job];
       uint32_t* sc = reinterpret_cast<uint32_t*>(scratch + gj.scratch);
       void* desc = h + gr.desc_off + q * sz;
-      if (gr.op == 0) {
+      if (gr.op == 2) {
+        std::memcpy(desc, p.few_desc.data() + gj.few, sz);
+      } else if (gr.op == 0) {
         afrs::EncodeArgs a{j.src, j.dst, j.shard_len, (int)j.n, (int)j.t, 0};
         afrs::fill_enc_job(desc, a, sc);
       } else {
@@ -1052,8 +1090,12 @@ cudaError_t batch_enqueue(afrs_ctx* c, const BatchPrep& p, uint8_t* d, cudaStrea
     for (size_t q = 0; q < order.size() && e == cudaSuccess; q++) {
       const BatchPrep::Group& gr = groups[order[q]];
       cudaStream_t gs = c->grp_stream[q % nstreams];
-      e = gr.op == 0 ? afrs::launch_encode_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs)
-                     : afrs::launch_recover_jobs(gr.n, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
+      if (gr.op == 0)
+        e = afrs::launch_encode_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
+      else if (gr.op == 1)
+        e = afrs::launch_recover_jobs(gr.n, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
+      else
+        e = afrs::launch_recover_few_jobs(gr.n, gr.t, d + gr.desc_off, (int)gr.count, gr.max_ncw, gs);
       *what = "batch group launch";
     }
   }

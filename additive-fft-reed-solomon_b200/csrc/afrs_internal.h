@@ -16,7 +16,8 @@ struct RecoverArgs {
   uint8_t pos[256];  // erased positions (first e entries)
   size_t pitch = 0;  // bytes between rows; 0 = L (the special kernels honour it)
   // n = 32 .. 128: kLayoutFused = one launch per call (the whole decoder per
-  // CTA), else the three phase kernels.
+  // CTA); n >= 32, e <= 8: kLayoutFew (or -1) = the few-erasure kernel;
+  // otherwise the three phase kernels.
   int layout = -1;
 };
 
@@ -34,6 +35,19 @@ struct EncodeArgs {
 };
 // Layout value of the one-launch form of the specialised kernels.
 constexpr int kLayoutFused = 2;
+// Layout value of the few-erasure recover (one pass over the survivors and an
+// e x e solve; n >= 32, 1 <= e <= 8).  With layout -1 the recover launcher
+// takes it wherever the shape allows.
+constexpr int kLayoutFew = 3;
+inline bool few_recover_shape(int n, int e) { return n >= 32 && n <= 256 && e >= 1 && e <= 8; }
+// Where a single call is faster on it than on the Leopard-form kernels
+// (B200, CUDA graphs): every n <= 128 (n = 64, 64 KiB shards: 4.6-9.4 vs
+// 16 us), and at n = 256, e <= 2, or e <= 4 with shards of 64 KiB or more
+// (1 MiB: e = 4 137 vs 272 us; 16 KiB: e = 4 22.2 vs 20.9 us; e = 8 loses
+// at every length: 64 KiB 36.7 vs 30.1 us).
+inline bool few_recover_wins(int n, int e, size_t L) {
+  return few_recover_shape(n, e) && (n <= 128 || e <= 2 || (e <= 4 && L >= 65536));
+}
 template <class A>
 __host__ __device__ inline size_t row_pitch(const A& a) {
   return a.pitch ? a.pitch : a.L;
@@ -78,7 +92,7 @@ cudaError_t launch_count_nonzero(const uint8_t* src, size_t len, unsigned long l
 // Per-call kernel routes (route.cu): the tuned table (route_table.inc,
 // written by tune.py) for a shape and shard-length bucket, or -1 when it has
 // no entry (the built-in rules decide).
-enum Route : int { kRouteGeneric = 0, kRouteSpecial = 1, kRouteSpecialSplit = 2, kRouteFused = 3 };
+enum Route : int { kRouteGeneric = 0, kRouteSpecial = 1, kRouteSpecialSplit = 2, kRouteFused = 3, kRouteFew = 4 };
 // Shapes the one-launch specialised form (kRouteFused) covers.
 inline bool fused_encode_shape(int n, int t) { return (t == 32 || t == 64) && t < n; }
 inline bool fused_recover_shape(int n) { return n >= 32 && n <= 128; }
@@ -117,11 +131,10 @@ cudaError_t ensure_smem_attr(const void* fn, size_t bytes);
 size_t scratch_bytes_recover(int n, size_t L);
 
 // Grouped launches of many codewords of one shape (afrs_batch_dev): op 0 =
-// encode, 1 = recover.  Each codeword gets a descriptor (job_desc_bytes,
-// filled on the host) and its own scratch (job_scratch_bytes, the whole
-// shard width); the descriptors are copied to device memory and launched per
-// shape group.  Supported for the phase-kernel shapes (encode t >= 32,
-// recover n >= 32).
+// encode, 1 = recover, 2 = few-erasure recover (n >= 32, e <= 8, no
+// scratch).  Each codeword gets a descriptor (job_desc_bytes, filled on the
+// host) and its own scratch (job_scratch_bytes, the whole shard width); the
+// descriptors are copied to device memory and launched per shape group.
 bool jobs_supported(int op, int n, int t);
 size_t job_desc_bytes(int op);
 size_t job_scratch_bytes(int op, int n, int t, size_t L);
@@ -130,5 +143,10 @@ void fill_enc_job(void* desc, const EncodeArgs& a, uint32_t* scratch);
 void fill_rec_job(void* desc, const RecoverArgs& a, uint32_t* scratch);
 cudaError_t launch_encode_jobs(int n, int t, const void* d_jobs, int count, size_t max_ncw, cudaStream_t s);
 cudaError_t launch_recover_jobs(int n, void* d_jobs, int count, size_t max_ncw, cudaStream_t s);
+// Few-erasure descriptor of one recover (the pattern's e x e solve, computed
+// here); false when the pattern has none (the job then takes op 1).
+bool fill_few_job(void* desc, const RecoverArgs& a);
+// A group of few-erasure recovers of one n, each with 2^logt / 2 < e <= 2^logt.
+cudaError_t launch_recover_few_jobs(int n, int logt, const void* d_jobs, int count, size_t max_ncw, cudaStream_t s);
 
 }  // namespace afrs

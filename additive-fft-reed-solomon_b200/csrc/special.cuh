@@ -1285,6 +1285,225 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_rec_b3_jobs(const RecJob* 
   rec_b3_body<LOGN>(j.a, Batch{j.s1, j.s2, j.ncw, 0}, blockIdx.x, blockIdx.z, st, j.loc);
 }
 
+// ---- recover, few erasures ------------------------------------------------
+// For 1 <= e <= 8 erasures: T = 2^ceil(log2 e) and the n/T chunks of T rows at
+// cosets omega_{iT}.  S = xor_i IFFT_T(chunk i, omega_{iT}) equals the top T
+// coefficients (n - T .. n - 1) of the word's polynomial in the LCH basis of
+// the Cantor basis: X_{uT + v} = X_{uT} X_v, X_{uT} is constant on each
+// chunk's coset, and its sum over the cosets is 1 for u = n/T - 1 and 0
+// below.  The decoder's output (rs/src/codec.rs:479-569, the Leopard form of
+// the phase kernels above) is the polynomial of degree < n - e through the
+// surviving rows, whose coefficients n - e .. n - 1 vanish.  With the erased
+// rows read as zero, S = S_known + V x over the erased values x, so
+// x = V_R^{-1} S_known[R] for the rows R = T - e .. T - 1 of S, on every input.
+// V_R^{-1} depends only on the erasure pattern and is computed on the host;
+// the kernel is one pass over the survivors (the chunk IFFTs of the t <= 16
+// encoder) and an e x e multiply by runtime constants, with no scratch.
+constexpr int kFewMax = 8;
+struct FewTable {
+  uint32_t er[8];    // erased rows, bit r of er[r / 32]
+  uint64_t m[8][8];  // output j, plane p: bit 8 r + q takes plane q of S[T - e + r]
+  uint8_t row[8];    // row of output j
+  int e;
+};
+
+inline int few_logt(int e) {
+  int l = 0;
+  while ((1 << l) < e) l++;
+  return l;
+}
+
+// IFFT of T = 2^logt bytes at coset beta: the map block_ifft applies to
+// bit-sliced rows (bf_inv: b ^= a, a ^= s_j(beta + omega_base) b).
+inline void host_ifft_bytes(uint8_t* v, int logt, uint8_t beta) {
+  const int T = 1 << logt;
+  for (int lv = 0; lv < logt; lv++)
+    for (int i = 0; i < T; i++) {
+      if ((i >> lv) & 1) continue;
+      const int j = i + (1 << lv);
+      const uint8_t tw = kField.spv[lv][static_cast<uint8_t>(beta ^ kField.omega[i & ~((2 << lv) - 1)])];
+      v[j] ^= v[i];
+      v[i] ^= gf_mul(tw, v[j]);
+    }
+}
+
+inline uint8_t host_gf_mul(uint8_t a, uint8_t b) {
+  return a && b ? kField.exp[kField.log[a] + kField.log[b]] : 0;
+}
+
+// The table of one erasure pattern; false when V_R is singular, which the
+// argument above rules out (the caller then runs the phase kernels).
+inline bool host_few_table(const RecoverArgs& a, FewTable* ft) {
+  const int e = a.e, lt = few_logt(e), T = 1 << lt, r0 = T - e;
+  *ft = FewTable{};
+  ft->e = e;
+  uint8_t aug[kFewMax][2 * kFewMax] = {};  // [V_R | I]
+  for (int j = 0; j < e; j++) {
+    const int p = a.pos[j];
+    ft->er[p >> 5] |= 1u << (p & 31);
+    ft->row[j] = static_cast<uint8_t>(p);
+    uint8_t u[kFewMax] = {};
+    u[p & (T - 1)] = 1;
+    host_ifft_bytes(u, lt, kField.omega[p & ~(T - 1)]);
+    for (int r = 0; r < e; r++) aug[r][j] = u[r0 + r];
+    aug[j][e + j] = 1;
+  }
+  for (int c = 0; c < e; c++) {  // Gauss-Jordan over GF(2^8)
+    int piv = c;
+    while (piv < e && !aug[piv][c]) piv++;
+    if (piv == e) return false;
+    if (piv != c)
+      for (int k = 0; k < 2 * e; k++) std::swap(aug[piv][k], aug[c][k]);
+    const uint8_t inv = kField.exp[255 - kField.log[aug[c][c]]];
+    for (int k = 0; k < 2 * e; k++) aug[c][k] = host_gf_mul(aug[c][k], inv);
+    for (int r = 0; r < e; r++) {
+      const uint8_t f = aug[r][c];
+      if (r == c || !f) continue;
+      for (int k = 0; k < 2 * e; k++) aug[r][k] ^= host_gf_mul(f, aug[c][k]);
+    }
+  }
+  // Coefficient b = V_R^{-1}[j][r]: byte q of `cols` is b * 2^q; after an 8x8
+  // bit transpose, byte p holds bit p of every b * 2^q, i.e. the planes q of
+  // S[r0 + r] that plane p of output j takes.
+  for (int j = 0; j < e; j++)
+    for (int r = 0; r < e; r++) {
+      uint8_t b = aug[j][e + r];
+      uint64_t cols = 0;
+      for (int q = 0; q < 8; q++) {
+        cols |= static_cast<uint64_t>(b) << (8 * q);
+        b = static_cast<uint8_t>((b << 1) ^ ((b & 0x80) ? 0x1d : 0));
+      }
+      uint64_t t = (cols ^ (cols >> 7)) & 0x00AA00AA00AA00AAull;
+      cols ^= t ^ (t << 7);
+      t = (cols ^ (cols >> 14)) & 0x0000CCCC0000CCCCull;
+      cols ^= t ^ (t << 14);
+      t = (cols ^ (cols >> 28)) & 0x00000000F0F0F0F0ull;
+      cols ^= t ^ (t << 28);
+      for (int p = 0; p < 8; p++) ft->m[j][p] |= ((cols >> (8 * p)) & 0xff) << (8 * r);
+    }
+  return true;
+}
+
+// Repeated calls with one erasure pattern (and the column windows of one
+// call) share a table: each host thread keeps its last one.  nullptr when
+// the pattern has none.
+inline const FewTable* cached_few_table(const RecoverArgs& a) {
+  thread_local FewTable t;
+  thread_local bool ok = false;
+  thread_local int e = -1;
+  thread_local uint8_t pos[kFewMax];
+  if (a.e != e || std::memcmp(pos, a.pos, (size_t)a.e) != 0) {
+    ok = host_few_table(a, &t);
+    e = a.e;
+    std::memcpy(pos, a.pos, (size_t)a.e);
+  }
+  return ok ? &t : nullptr;
+}
+
+// One CTA per 1024-column slice: its warps split the chunks (warp w takes
+// chunks w, w + 8, ...) and XOR-accumulate their IFFTs in shared memory; the
+// warps' rows are summed, then warp j computes erased row j.  With T = 1 the
+// chunk IFFT is the identity and the bit transpose is linear, so raw bytes
+// are XORed and transposed once.
+template <int LOGN, int LOGT>
+__device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTable& ft, unsigned bx, uint32_t* sm) {
+  constexpr int N = 1 << LOGN, T = 1 << LOGT, NC = N / T, W = kThreads / 32;
+  constexpr int WU = NC < W ? NC : W;
+  constexpr int kRows = T * 8 * 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if ((size_t)bx * 1024 >= a.L) return;  // the whole CTA
+  const size_t cw = (size_t)bx * 32 + lane;
+  const ShiftMul km = make_shift_mul();
+  const size_t pitch = row_pitch(a);
+  if (warp < WU) {
+    uint32_t acc[T][8];
+    zero_rows(acc);
+    for (int c = warp; c < NC; c += W) {
+      uint32_t x[T][8];
+#pragma unroll
+      for (int r = 0; r < T; r++) {
+        const int row = c * T + r;
+        if ((ft.er[row >> 5] >> (row & 31)) & 1u) {
+#pragma unroll
+          for (int p = 0; p < 8; p++) x[r][p] = 0;
+        } else if constexpr (LOGT == 0) {
+          load_cw(a.rx + (size_t)row * pitch, a.L, cw, x[r]);
+        } else {
+          gload(a.rx, row, pitch, a.L, cw, x[r], km);
+        }
+      }
+      if constexpr (LOGT > 0) {
+        dispatch<0, NC - 1>(c, [&](auto cc) {
+          constexpr int CC = decltype(cc)::value;
+          block_ifft<0, LOGT, 0, omega_c(CC * T), T>(x);
+        });
+      }
+#pragma unroll
+      for (int r = 0; r < T; r++)
+#pragma unroll
+        for (int p = 0; p < 8; p++) acc[r][p] ^= x[r][p];
+    }
+    if constexpr (LOGT == 0) transpose8f(acc[0], km);
+#pragma unroll
+    for (int r = 0; r < T; r++) sstore<32>(sm + warp * kRows, r, lane, acc[r]);
+  }
+  __syncthreads();
+  for (int r = warp; r < T; r += W) {
+    uint32_t y[8];
+    sload<32>(sm, r, lane, y);
+    for (int w = 1; w < WU; w++) {
+      uint32_t z[8];
+      sload<32>(sm + w * kRows, r, lane, z);
+#pragma unroll
+      for (int p = 0; p < 8; p++) y[p] ^= z[p];
+    }
+    sstore<32>(sm, r, lane, y);
+  }
+  __syncthreads();
+  if (warp >= ft.e) return;
+  const int r0 = T - ft.e;
+  uint32_t y[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int r = 0; r < T; r++) {
+    if (r < r0) continue;
+    uint32_t s[8];
+    sload<32>(sm, r, lane, s);
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+      const uint32_t mm = static_cast<uint32_t>(ft.m[warp][p] >> (8 * (r - r0)));
+#pragma unroll
+      for (int q = 0; q < 8; q++) y[p] ^= s[q] & (0u - ((mm >> q) & 1u));
+    }
+  }
+  gstore(a.rx, ft.row[warp], pitch, a.L, cw, y, km);
+}
+
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kThreads) k_rec_few(RecoverArgs a, const __grid_constant__ FewTable ft) {
+  extern __shared__ uint32_t sm[];
+  rec_few_body<LOGN, LOGT>(a, ft, blockIdx.x, sm);
+}
+
+template <int LOGN, int LOGT>
+constexpr size_t few_smem() {
+  constexpr int NC = (1 << LOGN) >> LOGT, W = kThreads / 32;
+  return (size_t)(NC < W ? NC : W) * (1 << LOGT) * 8 * 32 * 4;
+}
+
+// Grouped few-erasure recovers (afrs_batch_dev): codewords of one n and one
+// chunk size T, blockIdx.y = codeword, each with the table of its pattern.
+struct FewJob {
+  RecoverArgs a;
+  FewTable ft;
+};
+template <int LOGN, int LOGT>
+__global__ void __launch_bounds__(kThreads) k_rec_few_jobs(const FewJob* __restrict__ jobs) {
+  extern __shared__ uint32_t sm[];
+  const FewJob& j = jobs[blockIdx.y];
+  if ((size_t)blockIdx.x * 1024 >= j.a.L) return;
+  rec_few_body<LOGN, LOGT>(j.a, j.ft, blockIdx.x, sm);
+}
+
 // ---- launchers ------------------------------------------------------------
 
 // Launch that may start before the previous kernel on the stream has
@@ -1373,8 +1592,72 @@ cudaError_t launch_enc(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t
   }
 }
 
+template <int LOGN, int LOGT>
+cudaError_t launch_rec_few_t(const RecoverArgs& a, const FewTable& ft, cudaStream_t s) {
+  constexpr size_t smem = few_smem<LOGN, LOGT>();
+  if constexpr (smem > (48 << 10)) {
+    cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(k_rec_few<LOGN, LOGT>), smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_rec_few<LOGN, LOGT><<<(unsigned)((a.L + 1023) / 1024), kThreads, smem, s>>>(a, ft);
+  count_launches(1);
+  return cudaGetLastError();
+}
+template <int LOGN>
+cudaError_t launch_rec_few(const RecoverArgs& a, const FewTable& ft, cudaStream_t s) {
+  if (a.L == 0) return cudaSuccess;
+  switch (few_logt(a.e)) {
+    case 0: return launch_rec_few_t<LOGN, 0>(a, ft, s);
+    case 1: return launch_rec_few_t<LOGN, 1>(a, ft, s);
+    case 2: return launch_rec_few_t<LOGN, 2>(a, ft, s);
+    case 3: return launch_rec_few_t<LOGN, 3>(a, ft, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+template <int LOGN, int LOGT>
+cudaError_t launch_rec_few_jobs_t(const FewJob* d, int count, size_t max_ncw, cudaStream_t s) {
+  constexpr size_t smem = few_smem<LOGN, LOGT>();
+  if constexpr (smem > (48 << 10)) {
+    cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(k_rec_few_jobs<LOGN, LOGT>), smem);
+    if (e != cudaSuccess) return e;
+  }
+  const unsigned slices = (unsigned)((max_ncw + 31) / 32);
+  for (int j0 = 0; j0 < count; j0 += 65535) {
+    const unsigned cnt = (unsigned)(count - j0 < 65535 ? count - j0 : 65535);
+    k_rec_few_jobs<LOGN, LOGT><<<dim3(slices, cnt), kThreads, smem, s>>>(d + j0);
+    count_launches(1);
+  }
+  return cudaGetLastError();
+}
+// Every codeword of the group has 2^logt / 2 < e <= 2^logt erasures.
+template <int LOGN>
+cudaError_t launch_rec_few_jobs(const FewJob* d, int count, size_t max_ncw, int logt, cudaStream_t s) {
+  if constexpr (LOGN >= 5) {
+    if (count <= 0 || max_ncw == 0) return cudaSuccess;
+    switch (logt) {
+      case 0: return launch_rec_few_jobs_t<LOGN, 0>(d, count, max_ncw, s);
+      case 1: return launch_rec_few_jobs_t<LOGN, 1>(d, count, max_ncw, s);
+      case 2: return launch_rec_few_jobs_t<LOGN, 2>(d, count, max_ncw, s);
+      case 3: return launch_rec_few_jobs_t<LOGN, 3>(d, count, max_ncw, s);
+      default: return cudaErrorNotSupported;
+    }
+  } else {
+    return cudaErrorNotSupported;
+  }
+}
+
 template <int LOGN>
 cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s) {
+  if constexpr (LOGN >= 5) {
+    // Few erasures: one pass, no scratch (by default where it wins; layout 0
+    // or kLayoutFused keep the Leopard-form kernels).
+    if (((a.layout == kLayoutFew && few_recover_shape(1 << LOGN, a.e)) ||
+         (a.layout < 0 && few_recover_wins(1 << LOGN, a.e, a.L))) &&
+        (a.L + 1023) / 1024 <= 0x7fffffff) {
+      if (const FewTable* ft = cached_few_table(a)) return launch_rec_few<LOGN>(a, *ft, s);
+    }
+  }
   if constexpr (LOGN <= 4) {
     const size_t slices = (a.L + 1023) / 1024;
     k_rec_small<LOGN><<<(unsigned)((slices + 7) / 8), kThreads, 0, s>>>(a);
@@ -1504,6 +1787,10 @@ cudaError_t preload_rec() {
     cudaError_t e = cudaFuncGetAttributes(&fa, k_rec_b1<LOGN>);
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_p2<LOGN>);
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_b3<LOGN>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_few<LOGN, 0>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_few<LOGN, 1>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_few<LOGN, 2>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_rec_few<LOGN, 3>);
     return e;
   }
 }
@@ -1520,9 +1807,10 @@ inline size_t scratch_full_bytes_rec(int n, size_t L) { return n >= 32 ? (size_t
 #define AFRS_DECLARE_ENC(LN, LT)                                                                   \
   cudaError_t launch_enc_##LN##_##LT(const EncodeArgs& a, const ScratchArena& sc, cudaStream_t s); \
   cudaError_t launch_enc_jobs_##LN##_##LT(const EncJob* d, int count, size_t max_ncw, cudaStream_t s);
-#define AFRS_DECLARE_REC(LN)                                                                   \
-  cudaError_t launch_rec_##LN(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s); \
-  cudaError_t launch_rec_jobs_##LN(RecJob* d, int count, size_t max_ncw, cudaStream_t s);     \
+#define AFRS_DECLARE_REC(LN)                                                                          \
+  cudaError_t launch_rec_##LN(const RecoverArgs& a, const ScratchArena& sc, cudaStream_t s);        \
+  cudaError_t launch_rec_jobs_##LN(RecJob* d, int count, size_t max_ncw, cudaStream_t s);            \
+  cudaError_t launch_rec_few_jobs_##LN(const FewJob* d, int count, size_t max_ncw, int logt, cudaStream_t s); \
   cudaError_t preload_rec_##LN();
 AFRS_DECLARE_ENC(1, 0)
 AFRS_DECLARE_ENC(2, 0)

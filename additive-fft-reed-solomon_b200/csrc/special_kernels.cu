@@ -110,12 +110,16 @@ size_t scratch_bytes_recover(int n, size_t L) { return spec::scratch_full_bytes_
 
 // ---- grouped launches (afrs_batch_dev) --------------------------------------
 
-bool jobs_supported(int op, int n, int t) { return n >= 2 && n <= 256 && t >= 1 && t < n; }
+bool jobs_supported(int op, int n, int t) {
+  return n >= (op == 2 ? 32 : 2) && n <= 256 && t >= 1 && t < n;
+}
 
-size_t job_desc_bytes(int op) { return op == 0 ? sizeof(spec::EncJob) : sizeof(spec::RecJob); }
+size_t job_desc_bytes(int op) {
+  return op == 0 ? sizeof(spec::EncJob) : (op == 1 ? sizeof(spec::RecJob) : sizeof(spec::FewJob));
+}
 
 size_t job_scratch_bytes(int op, int n, int t, size_t L) {
-  return op == 0 ? spec::scratch_full_bytes_enc(n, t, L) : spec::scratch_full_bytes_rec(n, L);
+  return op == 0 ? spec::scratch_full_bytes_enc(n, t, L) : (op == 1 ? spec::scratch_full_bytes_rec(n, L) : 0);
 }
 
 size_t job_colwords(size_t L) { return spec::total_colwords(L); }
@@ -226,6 +230,25 @@ cudaError_t launch_recover_jobs(int n, void* d_jobs, int count, size_t max_ncw, 
     case 6: return spec::launch_rec_jobs_6(d, count, max_ncw, s);
     case 7: return spec::launch_rec_jobs_7(d, count, max_ncw, s);
     case 8: return spec::launch_rec_jobs_8(d, count, max_ncw, s);
+    default: return cudaErrorNotSupported;
+  }
+}
+
+bool fill_few_job(void* desc, const RecoverArgs& a) {
+  spec::FewJob j{};
+  j.a = a;
+  if (!spec::host_few_table(a, &j.ft)) return false;
+  std::memcpy(desc, &j, sizeof j);
+  return true;
+}
+
+cudaError_t launch_recover_few_jobs(int n, int logt, const void* d_jobs, int count, size_t max_ncw, cudaStream_t s) {
+  auto* d = static_cast<const spec::FewJob*>(d_jobs);
+  switch (__builtin_ctz((unsigned)n)) {
+    case 5: return spec::launch_rec_few_jobs_5(d, count, max_ncw, logt, s);
+    case 6: return spec::launch_rec_few_jobs_6(d, count, max_ncw, logt, s);
+    case 7: return spec::launch_rec_few_jobs_7(d, count, max_ncw, logt, s);
+    case 8: return spec::launch_rec_few_jobs_8(d, count, max_ncw, logt, s);
     default: return cudaErrorNotSupported;
   }
 }

@@ -211,7 +211,12 @@ int afrs_ctx_set_work_cap(afrs_ctx* ctx, size_t bytes);
  * splitting one slice's chunks (t <= 16 encodes with n > 2t; otherwise as
  * SPECIAL); FUSED, the compile-time-twiddle kernels in one launch per call,
  * one CTA holding every row of a 1024-column slice (encodes with t = 32 or
- * 64, recovers with n = 32 .. 128; otherwise as SPECIAL).  Results are
+ * 64, recovers with n = 32 .. 128; otherwise as SPECIAL); FEW, the
+ * few-erasure recover (n >= 32 and 1 <= e <= 8: one pass over the surviving
+ * shards and an e x e solve, no scratch; otherwise, and for encodes, as
+ * TABLE).  Under TABLE, recovers take FEW where it measured faster: n <= 128,
+ * and n = 256 with e <= 2, or e <= 4 and shards of 64 KiB or more; batches
+ * (afrs_batch_dev) give it every recover it covers.  Results are
  * identical on every route.  No counterpart in the reference, whose kernel
  * choice is a build-time CPU feature test (rs/build.rs:628-646). */
 #define AFRS_ROUTE_TABLE 0
@@ -219,6 +224,7 @@ int afrs_ctx_set_work_cap(afrs_ctx* ctx, size_t bytes);
 #define AFRS_ROUTE_SPECIAL 2
 #define AFRS_ROUTE_SPECIAL_SPLIT 3
 #define AFRS_ROUTE_FUSED 4
+#define AFRS_ROUTE_FEW 5
 int afrs_ctx_set_route(afrs_ctx* ctx, int route);
 
 /* Number of CUDA kernels this library has launched in this process, over

@@ -10,7 +10,7 @@ from oracle import oracle
 torch = pytest.importorskip("torch")
 
 ROUTES = ["AFRS_ROUTE_TABLE", "AFRS_ROUTE_GENERIC", "AFRS_ROUTE_SPECIAL", "AFRS_ROUTE_SPECIAL_SPLIT",
-          "AFRS_ROUTE_FUSED"]
+          "AFRS_ROUTE_FUSED", "AFRS_ROUTE_FEW"]
 
 
 def test_set_route_argument_checks(afrs):
@@ -22,7 +22,7 @@ def test_set_route_argument_checks(afrs):
 def test_set_route_rejects_unknown_values(afrs):
     ctx = afrs.Context(0)
     with pytest.raises(afrs.AfrsError):
-        ctx.set_route(5)
+        ctx.set_route(6)
     with pytest.raises(afrs.AfrsError):
         ctx.set_route(-1)
     ctx.close()
