@@ -41,12 +41,12 @@ constexpr int kLayoutFused = 2;
 constexpr int kLayoutFew = 3;
 inline bool few_recover_shape(int n, int e) { return n >= 32 && n <= 256 && e >= 1 && e <= 8; }
 // Where a single call is faster on it than on the Leopard-form kernels
-// (B200, CUDA graphs): every n <= 128 (n = 64, 64 KiB shards: 4.6-9.4 vs
-// 16 us), and at n = 256, e <= 2, or e <= 4 with shards of 64 KiB or more
-// (1 MiB: e = 4 137 vs 272 us; 16 KiB: e = 4 22.2 vs 20.9 us; e = 8 loses
-// at every length: 64 KiB 36.7 vs 30.1 us).
+// (B200, CUDA graphs): every n <= 128 (n = 64, 64 KiB shards: 4.5-10.1 vs
+// 16 us), and at n = 256, e <= 2, e <= 4 with shards of 64 KiB or more, or
+// any e <= 8 from 1 MiB (1 MiB: e = 4 134 vs 272 us, e = 8 195 vs 300;
+// 16 KiB: e = 4 21.2 vs 20.9 us; 64 KiB: e = 8 40 vs 30 us).
 inline bool few_recover_wins(int n, int e, size_t L) {
-  return few_recover_shape(n, e) && (n <= 128 || e <= 2 || (e <= 4 && L >= 65536));
+  return few_recover_shape(n, e) && (n <= 128 || e <= 2 || (e <= 4 && L >= 65536) || L >= ((size_t)1 << 20));
 }
 template <class A>
 __host__ __device__ inline size_t row_pitch(const A& a) {

@@ -1415,8 +1415,12 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
   const size_t cw = (size_t)bx * 32 + lane;
   const ShiftMul km = make_shift_mul();
   const size_t pitch = row_pitch(a);
+  // T = 8 accumulates in the warp's shared-memory rows, so that two CTAs
+  // fit an SM (at most 128 registers).
+  constexpr bool kSmemAcc = LOGT >= 3;
   if (warp < WU) {
-    uint32_t acc[T][8];
+    uint32_t* wacc = sm + warp * kRows;
+    uint32_t acc[kSmemAcc ? 1 : T][8];
     zero_rows(acc);
     for (int c = warp; c < NC; c += W) {
       uint32_t x[T][8];
@@ -1438,14 +1442,30 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
           block_ifft<0, LOGT, 0, omega_c(CC * T), T>(x);
         });
       }
+      if constexpr (kSmemAcc) {
+        const bool first = c == warp;
 #pragma unroll
-      for (int r = 0; r < T; r++)
+        for (int r = 0; r < T; r++) {
+          if (!first) {
+            uint32_t y[8];
+            sload<32>(wacc, r, lane, y);
 #pragma unroll
-        for (int p = 0; p < 8; p++) acc[r][p] ^= x[r][p];
+            for (int p = 0; p < 8; p++) x[r][p] ^= y[p];
+          }
+          sstore<32>(wacc, r, lane, x[r]);
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < T; r++)
+#pragma unroll
+          for (int p = 0; p < 8; p++) acc[r][p] ^= x[r][p];
+      }
     }
-    if constexpr (LOGT == 0) transpose8f(acc[0], km);
+    if constexpr (!kSmemAcc) {
+      if constexpr (LOGT == 0) transpose8f(acc[0], km);
 #pragma unroll
-    for (int r = 0; r < T; r++) sstore<32>(sm + warp * kRows, r, lane, acc[r]);
+      for (int r = 0; r < T; r++) sstore<32>(wacc, r, lane, acc[r]);
+    }
   }
   __syncthreads();
   for (int r = warp; r < T; r += W) {
@@ -1478,8 +1498,12 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
   gstore(a.rx, ft.row[warp], pitch, a.L, cw, y, km);
 }
 
+// CTAs per SM the few-erasure kernels are compiled for (register caps 64,
+// 85, 128, 128 for T = 1, 2, 4, 8; without caps ptxas takes up to 174).
+constexpr int few_min_ctas(int logt) { return logt == 0 ? 4 : (logt == 1 ? 3 : 2); }
+
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kThreads) k_rec_few(RecoverArgs a, const __grid_constant__ FewTable ft) {
+__global__ void __launch_bounds__(kThreads, few_min_ctas(LOGT)) k_rec_few(RecoverArgs a, const __grid_constant__ FewTable ft) {
   extern __shared__ uint32_t sm[];
   rec_few_body<LOGN, LOGT>(a, ft, blockIdx.x, sm);
 }
@@ -1497,7 +1521,7 @@ struct FewJob {
   FewTable ft;
 };
 template <int LOGN, int LOGT>
-__global__ void __launch_bounds__(kThreads) k_rec_few_jobs(const FewJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kThreads, few_min_ctas(LOGT)) k_rec_few_jobs(const FewJob* __restrict__ jobs) {
   extern __shared__ uint32_t sm[];
   const FewJob& j = jobs[blockIdx.y];
   if ((size_t)blockIdx.x * 1024 >= j.a.L) return;

@@ -348,12 +348,13 @@ def run_kernels(args):
                      "GB/s": round(n * L / ms / 1e6, 1), "bit_exact": ok}
         ctx.close()
 
-    def recover_case(name, n, t, L, route, kernels):
+    def recover_case(name, n, t, L, route, kernels, e=None):
+        e = t if e is None else e
         msg = oracle.random_bytes((n - t) * L, n * 7 + t)
         par = np.zeros(t * L, np.uint8)
         oracle.encode_systematic_sharded(n, t, msg, par, L)
         cw = np.concatenate([par, msg])
-        pos = sorted(np.random.default_rng(n).choice(n, t, replace=False).tolist())
+        pos = sorted(np.random.default_rng(n).choice(n, e, replace=False).tolist())
         rx = cw.copy()
         for p in pos:
             rx[p * L:(p + 1) * L] = 0
@@ -363,7 +364,7 @@ def run_kernels(args):
         d = torch.from_numpy(rx).cuda()
         ms = timed(lambda: codec.recover_erasure_shards(d, None, L, pos))
         ok = bool((d.cpu().numpy() == cw).all())
-        out[name] = {"n": n, "t": t, "e": t, "L": L, "kernels": kernels, "us": round(ms * 1e3, 2),
+        out[name] = {"n": n, "t": t, "e": e, "L": L, "kernels": kernels, "us": round(ms * 1e3, 2),
                      "GB/s": round(n * L / ms / 1e6, 1), "bit_exact": ok}
         ctx.close()
 
@@ -378,6 +379,10 @@ def run_kernels(args):
     recover_case("recover_fused_n32", 32, 16, 524288, lib.AFRS_ROUTE_FUSED, "k_rec_fused<5>")
     recover_case("recover_fused_n64", 64, 32, 262144, lib.AFRS_ROUTE_FUSED, "k_rec_fused<6>")
     recover_case("recover_phases_n32", 32, 16, 524288, lib.AFRS_ROUTE_SPECIAL, "k_rec_b1/p2/b3<5>")
+    recover_case("recover_few_n256_e1", 256, 8, 65536, lib.AFRS_ROUTE_FEW, "k_rec_few<8,0>", e=1)
+    recover_case("recover_few_n256_e8", 256, 8, 65536, lib.AFRS_ROUTE_FEW, "k_rec_few<8,3>", e=8)
+    recover_case("recover_few_n64_e4", 64, 8, 262144, lib.AFRS_ROUTE_FEW, "k_rec_few<6,2>", e=4)
+    recover_case("recover_phases_n256_e8", 256, 8, 65536, lib.AFRS_ROUTE_SPECIAL, "k_rec_b1/p2/b3<8>", e=8)
 
     # Batched path: 256 small mixed jobs share the generic persistent kernel
     # (every shape group is below the grouping threshold); two large shape

@@ -215,7 +215,8 @@ int afrs_ctx_set_work_cap(afrs_ctx* ctx, size_t bytes);
  * few-erasure recover (n >= 32 and 1 <= e <= 8: one pass over the surviving
  * shards and an e x e solve, no scratch; otherwise, and for encodes, as
  * TABLE).  Under TABLE, recovers take FEW where it measured faster: n <= 128,
- * and n = 256 with e <= 2, or e <= 4 and shards of 64 KiB or more; batches
+ * and n = 256 with e <= 2, e <= 4 and shards of 64 KiB or more, or shards of
+ * 1 MiB or more; batches
  * (afrs_batch_dev) give it every recover it covers.  Results are
  * identical on every route.  No counterpart in the reference, whose kernel
  * choice is a build-time CPU feature test (rs/build.rs:628-646). */
