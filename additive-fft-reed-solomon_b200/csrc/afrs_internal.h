@@ -41,13 +41,10 @@ constexpr int kLayoutFused = 2;
 constexpr int kLayoutFew = 3;
 inline bool few_recover_shape(int n, int e) { return n >= 32 && n <= 256 && e >= 1 && e <= 8; }
 // Where a single call is faster on it than on the Leopard-form kernels
-// (B200, CUDA graphs): every n <= 128 (n = 64, 64 KiB shards: 4.5-10.1 vs
-// 16 us), and at n = 256, e <= 2, e <= 4 with shards of 64 KiB or more, or
-// any e <= 8 from 1 MiB (1 MiB: e = 4 134 vs 272 us, e = 8 195 vs 300;
-// 16 KiB: e = 4 21.2 vs 20.9 us; 64 KiB: e = 8 40 vs 30 us).
-inline bool few_recover_wins(int n, int e, size_t L) {
-  return few_recover_shape(n, e) && (n <= 128 || e <= 2 || (e <= 4 && L >= 65536) || L >= ((size_t)1 << 20));
-}
+// (B200, CUDA graphs): every shape it covers, at every measured shard length
+// (1 KiB .. 1 MiB; n = 256, 64 KiB shards: e = 1 7.8 vs 28.2 us, e = 8 27.8
+// vs 30.1; 1 KiB, e = 8: 16.4 vs 16.5).
+inline bool few_recover_wins(int n, int e, size_t) { return few_recover_shape(n, e); }
 template <class A>
 __host__ __device__ inline size_t row_pitch(const A& a) {
   return a.pitch ? a.pitch : a.L;

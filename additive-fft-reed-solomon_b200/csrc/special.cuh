@@ -26,6 +26,8 @@
 // where it measured faster (short shards).
 // Transforms with k <= 4 run entirely inside one thread.
 #pragma once
+#include <cooperative_groups.h>
+
 #include <array>
 #include <cstring>
 #include <utility>
@@ -1400,18 +1402,22 @@ inline const FewTable* cached_few_table(const RecoverArgs& a) {
   return ok ? &t : nullptr;
 }
 
-// One CTA per 1024-column slice: its warps split the chunks (warp w takes
-// chunks w, w + 8, ...) and XOR-accumulate their IFFTs in shared memory; the
-// warps' rows are summed, then warp j computes erased row j.  With T = 1 the
-// chunk IFFT is the identity and the bit transpose is linear, so raw bytes
-// are XORed and transposed once.
+// One CTA, or a cluster of nc CTAs, per 1024-column slice: the cluster's
+// warps split the chunks (warp g = rank * 8 + w takes chunks g, g + 8 nc,
+// ...) and XOR-accumulate their IFFTs in shared memory; each CTA sums its
+// warps' rows, CTA 0 adds the other CTAs' sums through distributed shared
+// memory, then its warp j computes erased row j.  With T = 1 the chunk IFFT
+// is the identity and the bit transpose is linear, so raw bytes are XORed and
+// transposed once.  Clusters give short shards (few slices) more SMs.
 template <int LOGN, int LOGT>
-__device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTable& ft, unsigned bx, uint32_t* sm) {
+__device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTable& ft, unsigned bx, unsigned rank,
+                                             unsigned nc, uint32_t* sm) {
   constexpr int N = 1 << LOGN, T = 1 << LOGT, NC = N / T, W = kThreads / 32;
-  constexpr int WU = NC < W ? NC : W;
   constexpr int kRows = T * 8 * 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if ((size_t)bx * 1024 >= a.L) return;  // the whole CTA
+  if ((size_t)bx * 1024 >= a.L) return;  // the whole CTA (the whole cluster: bx is shared)
+  const int g0 = (int)rank * W;            // this CTA's first warp in the cluster
+  const int WU = NC - g0 < W ? (NC - g0 > 0 ? NC - g0 : 0) : W;  // its warps that get chunks
   const size_t cw = (size_t)bx * 32 + lane;
   const ShiftMul km = make_shift_mul();
   const size_t pitch = row_pitch(a);
@@ -1422,7 +1428,7 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
     uint32_t* wacc = sm + warp * kRows;
     uint32_t acc[kSmemAcc ? 1 : T][8];
     zero_rows(acc);
-    for (int c = warp; c < NC; c += W) {
+    for (int c = g0 + warp; c < NC; c += W * (int)nc) {
       uint32_t x[T][8];
 #pragma unroll
       for (int r = 0; r < T; r++) {
@@ -1443,7 +1449,7 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
         });
       }
       if constexpr (kSmemAcc) {
-        const bool first = c == warp;
+        const bool first = c == g0 + warp;
 #pragma unroll
         for (int r = 0; r < T; r++) {
           if (!first) {
@@ -1469,9 +1475,8 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
   }
   __syncthreads();
   for (int r = warp; r < T; r += W) {
-    uint32_t y[8];
-    sload<32>(sm, r, lane, y);
-    for (int w = 1; w < WU; w++) {
+    uint32_t y[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int w = 0; w < WU; w++) {
       uint32_t z[8];
       sload<32>(sm + w * kRows, r, lane, z);
 #pragma unroll
@@ -1479,7 +1484,30 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
     }
     sstore<32>(sm, r, lane, y);
   }
-  __syncthreads();
+  if (nc > 1) {
+    // Every CTA's sums are in its region 0; CTA 0 reads the others' (their
+    // shared memory stays live until the second barrier).
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    if (rank == 0) {
+      for (int r = warp; r < T; r += W) {
+        uint32_t y[8];
+        sload<32>(sm, r, lane, y);
+        for (unsigned k = 1; k < nc; k++) {
+          uint32_t z[8];
+          sload<32>(cluster.map_shared_rank(sm, k), r, lane, z);
+#pragma unroll
+          for (int p = 0; p < 8; p++) y[p] ^= z[p];
+        }
+        sstore<32>(sm, r, lane, y);
+      }
+    }
+    cluster.sync();
+    if (rank != 0) return;
+  } else {
+    __syncthreads();
+  }
   if (warp >= ft.e) return;
   const int r0 = T - ft.e;
   uint32_t y[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1505,7 +1533,8 @@ constexpr int few_min_ctas(int logt) { return logt == 0 ? 4 : (logt == 1 ? 3 : 2
 template <int LOGN, int LOGT>
 __global__ void __launch_bounds__(kThreads, few_min_ctas(LOGT)) k_rec_few(RecoverArgs a, const __grid_constant__ FewTable ft) {
   extern __shared__ uint32_t sm[];
-  rec_few_body<LOGN, LOGT>(a, ft, blockIdx.x, sm);
+  const unsigned nc = cooperative_groups::this_cluster().num_blocks();
+  rec_few_body<LOGN, LOGT>(a, ft, blockIdx.x / nc, blockIdx.x % nc, nc, sm);
 }
 
 template <int LOGN, int LOGT>
@@ -1525,7 +1554,7 @@ __global__ void __launch_bounds__(kThreads, few_min_ctas(LOGT)) k_rec_few_jobs(c
   extern __shared__ uint32_t sm[];
   const FewJob& j = jobs[blockIdx.y];
   if ((size_t)blockIdx.x * 1024 >= j.a.L) return;
-  rec_few_body<LOGN, LOGT>(j.a, j.ft, blockIdx.x, sm);
+  rec_few_body<LOGN, LOGT>(j.a, j.ft, blockIdx.x, 0, 1, sm);
 }
 
 // ---- launchers ------------------------------------------------------------
@@ -1623,9 +1652,31 @@ cudaError_t launch_rec_few_t(const RecoverArgs& a, const FewTable& ft, cudaStrea
     cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(k_rec_few<LOGN, LOGT>), smem);
     if (e != cudaSuccess) return e;
   }
-  k_rec_few<LOGN, LOGT><<<(unsigned)((a.L + 1023) / 1024), kThreads, smem, s>>>(a, ft);
+  // Clusters of up to 8 CTAs per slice while the slices alone would leave
+  // SMs idle (below two CTAs per SM), each warp keeping at least one chunk
+  // and four rows (n = 32 and 64 measured slower with smaller shares: the
+  // cluster barriers cost more than the rows); one CTA per slice otherwise.
+  const size_t slices = (a.L + 1023) / 1024;
+  constexpr unsigned kChunkCap = (unsigned)(((1 << LOGN) >> LOGT) + kThreads / 32 - 1) / (kThreads / 32);
+  constexpr unsigned kRowCap = (1u << LOGN) / 32;
+  constexpr unsigned kCap = kChunkCap < kRowCap ? kChunkCap : kRowCap;
+  unsigned nc = 1;
+  while (nc < 8 && 2 * nc <= kCap && slices * nc < 2 * 148) nc *= 2;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(slices * nc));
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = nc;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k_rec_few<LOGN, LOGT>, a, ft);
   count_launches(1);
-  return cudaGetLastError();
+  return e;
 }
 template <int LOGN>
 cudaError_t launch_rec_few(const RecoverArgs& a, const FewTable& ft, cudaStream_t s) {

@@ -214,10 +214,9 @@ int afrs_ctx_set_work_cap(afrs_ctx* ctx, size_t bytes);
  * 64, recovers with n = 32 .. 128; otherwise as SPECIAL); FEW, the
  * few-erasure recover (n >= 32 and 1 <= e <= 8: one pass over the surviving
  * shards and an e x e solve, no scratch; otherwise, and for encodes, as
- * TABLE).  Under TABLE, recovers take FEW where it measured faster: n <= 128,
- * and n = 256 with e <= 2, e <= 4 and shards of 64 KiB or more, or shards of
- * 1 MiB or more; batches
- * (afrs_batch_dev) give it every recover it covers.  Results are
+ * TABLE).  Under TABLE (and in batches, afrs_batch_dev) every recover FEW
+ * covers takes it: it measured faster than the other families at every such
+ * shape and shard length.  Results are
  * identical on every route.  No counterpart in the reference, whose kernel
  * choice is a build-time CPU feature test (rs/build.rs:628-646). */
 #define AFRS_ROUTE_TABLE 0

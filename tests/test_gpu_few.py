@@ -89,9 +89,9 @@ def test_few_edge_patterns(afrs, n, t, pos):
 @pytest.mark.gpu
 def test_few_is_one_launch_and_falls_back_beyond_eight(afrs):
     lib = afrs.lib()
-    # n = 256 takes it for e <= 2 (e <= 4 from 64 KiB, e <= 8 from 1 MiB), n <= 128
-    # for every e <= 8; beyond, the three Leopard-form phase kernels.
-    for n, e, launches in ((256, 1, 1), (256, 2, 1), (256, 8, 3), (128, 8, 1), (128, 9, 3)):
+    # Every n >= 32 takes it for e <= 8; beyond, the three Leopard-form phase
+    # kernels.
+    for n, e, launches in ((256, 1, 1), (256, 2, 1), (256, 8, 1), (128, 8, 1), (128, 9, 3), (256, 9, 3)):
         t, L = 32, 4096
         cw = _codeword(n, t, L, seed=5 + n)
         pos = list(range(40, 40 + e))
