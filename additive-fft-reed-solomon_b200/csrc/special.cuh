@@ -1786,8 +1786,11 @@ cudaError_t launch_rec(const RecoverArgs& a, const ScratchArena& sc, cudaStream_
 template <int LOGN, int LOGT>
 cudaError_t launch_enc_jobs(const EncJob* d, int count, size_t max_ncw, cudaStream_t s) {
   if constexpr (LOGT <= 4) {
+    // The layout rule counts the slices of the whole group: many codewords
+    // fill the GPU as slices do (t = 16: one warp per slice once the group
+    // holds more than 128).
     const size_t slices = (max_ncw + 31) / 32;
-    const bool split = enc_small_split<LOGN, LOGT>(slices);
+    const bool split = enc_small_split<LOGN, LOGT>(slices * (size_t)count);
     const size_t smem = enc_small_smem<LOGN, LOGT>(split);
     auto fn = split ? k_enc_small_jobs<LOGN, LOGT, true> : k_enc_small_jobs<LOGN, LOGT, false>;
     if (smem > (48 << 10)) {

@@ -156,3 +156,25 @@ def test_t16_encode_group_of_a_batch(afrs, n):
     assert afrs.run_batch(jobs) == [0, 0]
     for j, ref in zip(jobs, refs):
         assert (j.dst.cpu().numpy() == ref).all()
+
+
+@pytest.mark.gpu
+def test_t16_encode_group_of_many_short_codewords(afrs):
+    """A t = 16 group of many short, ragged codewords (more than 128 slices
+    in the group, at most 5 per codeword) also takes the one-warp-per-slice
+    grouped kernel; each codeword's parity equals the oracle's."""
+    n, t = 64, 16
+    rng = np.random.default_rng(16)
+    jobs, refs = [], []
+    for i in range(60):
+        L = int(rng.choice([1000, 3001, 4096, 5000]))
+        msg = oracle.random_bytes((n - t) * L, 900 + i)
+        ref = np.zeros(t * L, np.uint8)
+        oracle.encode_systematic_sharded(n, t, msg, ref, L)
+        jobs.append(afrs.Job.encode(n, t, torch.from_numpy(msg).cuda(),
+                                    torch.full((t * L,), 0x5A, dtype=torch.uint8, device="cuda"), L))
+        refs.append(ref)
+    assert sum(j.nbytes for j in jobs) >= 8 << 20
+    assert afrs.run_batch(jobs) == [0] * len(jobs)
+    for j, ref in zip(jobs, refs):
+        assert (j.dst.cpu().numpy() == ref).all()
