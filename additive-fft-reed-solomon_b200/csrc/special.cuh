@@ -1520,7 +1520,8 @@ __device__ __forceinline__ void rec_few_body(const RecoverArgs& a, const FewTabl
     for (int p = 0; p < 8; p++) {
       const uint32_t mm = static_cast<uint32_t>(ft.m[warp][p] >> (8 * (r - r0)));
 #pragma unroll
-      for (int q = 0; q < 8; q++) y[p] ^= s[q] & (0u - ((mm >> q) & 1u));
+      for (int q = 0; q < 8; q++)
+        if ((mm >> q) & 1u) y[p] ^= s[q];  // warp-uniform: a predicated XOR
     }
   }
   gstore(a.rx, ft.row[warp], pitch, a.L, cw, y, km);
