@@ -718,8 +718,13 @@ int afrs_recover(afrs_ctx* c, uint32_t n, uint32_t t, uint8_t* received, size_t 
   if (drx) {
     a.rx = drx;
     a.L = L;
+    // The few-erasure kernel, which the launcher takes where it wins, needs
+    // no scratch.
     r = run_direct(
-        c, a, [&](size_t W) { return afrs::scratch_bytes_recover((int)n, W); },
+        c, a,
+        [&](size_t W) {
+          return afrs::few_recover_wins((int)n, (int)e_count, W) ? 0 : afrs::scratch_bytes_recover((int)n, W);
+        },
         [](afrs::RecoverArgs& w, size_t c0) { w.rx += c0; },
         [](const afrs::RecoverArgs& w, const afrs::ScratchArena& sc, cudaStream_t s) {
           return afrs::launch_recover_special(w, sc, s);
