@@ -234,21 +234,30 @@ __device__ __forceinline__ void enc_small_split_body(const EncodeArgs& a, unsign
     sstore<32>(sm, r, lane, y);
   }
   __syncthreads();
-  if (warp != 0) return;
-  uint32_t f[T][8];
+  // Warp 0 runs the final FFT; the warps then transpose and store one parity
+  // row each (warp 0 alone storing all T rows was the CTA's serial tail).
+  if (warp == 0) {
+    uint32_t f[T][8];
 #pragma unroll
-  for (int r = 0; r < T; r++) {
-    sload<32>(sm, r, lane, f[r]);
-    if (a.accumulate) {
-      uint32_t y[8];
-      gload(a.parity, r, row_pitch(a), a.L, cw, y, km);
+    for (int r = 0; r < T; r++) {
+      sload<32>(sm, r, lane, f[r]);
+      if (a.accumulate) {
+        uint32_t y[8];
+        gload(a.parity, r, row_pitch(a), a.L, cw, y, km);
 #pragma unroll
-      for (int p = 0; p < 8; p++) f[r][p] ^= y[p];
+        for (int p = 0; p < 8; p++) f[r][p] ^= y[p];
+      }
     }
-  }
-  block_fft<0, LOGT, 0, 0, T>(f);
+    block_fft<0, LOGT, 0, 0, T>(f);
 #pragma unroll
-  for (int r = 0; r < T; r++) gstore(a.parity, r, row_pitch(a), a.L, cw, f[r], km);
+    for (int r = 0; r < T; r++) sstore<32>(sm, r, lane, f[r]);
+  }
+  __syncthreads();
+  for (int r = warp; r < T; r += W) {
+    uint32_t y[8];
+    sload<32>(sm, r, lane, y);
+    gstore(a.parity, r, row_pitch(a), a.L, cw, y, km);
+  }
 }
 
 // Layout of the t <= 16 encode.  With more than one chunk and few slices of
