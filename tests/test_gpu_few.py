@@ -203,3 +203,42 @@ def test_few_batch_groups_match_oracle(afrs):
         for j, ex, st in zip(jobs, expect, status):
             assert st == 1
             assert (j.dst.cpu().numpy() == ex).all(), (j.n, j.t, len(j.positions), j.shard_len)
+
+
+@pytest.mark.gpu
+def test_few_from_concurrent_threads_with_different_patterns(afrs):
+    """Host threads recovering different few-erasure patterns at once (each
+    thread keeps its own cached solve; pageable and page-locked buffers,
+    device buffers on its own context) give the oracle's bytes every time."""
+    import threading
+
+    n, t, L, steps = 128, 16, 6000, 5
+    cw = _codeword(n, t, L, seed=77)
+    rng = np.random.default_rng(12)
+    patterns = [sorted(rng.choice(n, e, replace=False).tolist()) for e in (1, 3, 5, 8, 2, 7)]
+    errors = []
+
+    def work(q, pos):
+        try:
+            codec = afrs.Codec(n, t, context=afrs.Context(0))
+            for s in range(steps):
+                p = pos if s % 2 == 0 else patterns[(q + 1) % len(patterns)]
+                rx = _erase(cw, L, p)
+                if q % 3 == 0:
+                    buf = rx
+                elif q % 3 == 1:
+                    buf = torch.from_numpy(rx).pin_memory().numpy()
+                else:
+                    buf = torch.from_numpy(rx).cuda()
+                assert codec.recover_erasure_shards(buf, None, L, p)
+                out = buf.cpu().numpy() if isinstance(buf, torch.Tensor) else buf
+                assert (out == cw).all(), (q, s)
+        except Exception as ex:  # surfaced below
+            errors.append(ex)
+
+    ths = [threading.Thread(target=work, args=(q, p)) for q, p in enumerate(patterns)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    assert not errors, errors[0]
