@@ -38,7 +38,7 @@ def _noalloc(afrs, n, t, d_rx, L, pos):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,t,L", [(256, 128, 65536), (256, 32, 5000), (64, 32, 1024), (16, 8, 333)])
+@pytest.mark.parametrize("n,t,L", [(256, 128, 65536), (256, 32, 5000), (64, 32, 1024), (16, 8, 333), (128, 8, 3000)])
 def test_noalloc_matches_regular_entry_point_twice(afrs, n, t, L):
     rng = np.random.default_rng(n + t + L)
     codec = afrs.Codec(n, t)
